@@ -1,0 +1,339 @@
+#!/usr/bin/env python3
+"""Headline benchmark: bulk insert & lookup Mops/s at LF 0.9 with 2^26 slots on B200.
+
+One step = clear the table, bulk-insert n = floor(0.9 * 2^26) = 60,397,977 unique keys with their
+values, then bulk-look-up n keys of which half are present (sampled from the inserted keys) and
+half absent, shuffled.  Keys: splitmix64 seed 7 (hivehashtable_b200/csrc/hive_workload.cpp).
+value = 2n * steps / time over all ranks (Mops/s); every input is resident in HBM before timing
+and is larger than the 126 MB L2 (table 512 MiB, key arrays 241 MB each).
+
+`e2e` times the same step through the public API from pinned host buffers, with the host->device
+copies of keys/values/lookup keys and the device->host copies of statuses/found flags/values
+inside the timed region.  `cpu_baseline` / `--impl reference` time the CPU port of the same
+algorithm (oracle/hive_oracle.cpp, std::thread on every host core) on a bounded sample.
+
+Multi-GPU (torchrun): each rank owns an independent table with its own keys (seed 7 + 1000*rank);
+there is no data-path collective, so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "bulk insert & lookup Mops/s at LF 0.9, 2^26 keys"
+UNIT = "Mops/s"
+# Algorithmic bytes per op (32 B sectors; 64 B bucket): insert of a new key reads its two
+# candidate buckets (128 B), writes one sector (32 B), streams key+value in (8 B) and a status
+# out (4 B) = 172 B; lookup present = 64 + 4 + 8 = 76 B, absent = 128 + 4 + 8 = 140 B.
+BYTES_INSERT = 172.0
+BYTES_LOOKUP_PRESENT = 76.0
+BYTES_LOOKUP_ABSENT = 140.0
+# DRAM bytes per op measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum per launch / ops)
+# for k_insert and k_find at this workload; profiles/k_insert_k_find_ncu_2p26_lf09.txt.
+TRAFFIC_PER_OP = {"insert": None, "lookup": None}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["hive", "reference"], default="hive")
+    ap.add_argument("--policy", default="Default2Hash")
+    ap.add_argument("--cap-log", type=int, default=26)
+    ap.add_argument("--lf", type=float, default=0.9)
+    ap.add_argument("--present", type=float, default=0.5)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample-log", type=int, default=24, help="log2 slots of the CPU-baseline sample")
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for ln in out.stdout.strip().splitlines():
+                    self.rows.append([c.strip() for c in ln.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def cpu_baseline(args, threads=None):
+    """The CPU port of the same algorithm (oracle/hive_oracle.cpp) on every host core: a bounded
+    sample with the headline's LF and present fraction at 2^cpu_sample_log slots."""
+    import oracle
+    from hivehashtable_b200 import workload
+
+    threads = threads or oracle.host_threads()
+    cap = 1 << args.cpu_sample_log
+    n = int(args.lf * cap)
+    keys, vals, look = workload.bulk_workload(args.seed, n, args.present)
+    t = oracle.CpuTable(0 if args.policy == "Default2Hash" else 1, cap)
+    _, ti = t.insert(keys, vals, threads)
+    _, f, tf = t.find(look, threads)
+    del t
+    mops = 2 * n / (ti + tf) / 1e6
+    return {"value": round(mops, 2), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} inserts into 2^{args.cpu_sample_log} slots (LF {args.lf}) + {n} lookups "
+                      f"({args.present:.0%} present), std::thread x {threads}",
+            "insert_mops": round(n / ti / 1e6, 2), "lookup_mops": round(n / tf / 1e6, 2),
+            "seconds": round(ti + tf, 3)}
+
+
+def run_reference(args, rank, world):
+    line = {"metric": METRIC, "impl": "reference", "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic"}
+    if rank != 0:
+        return None
+    for _ in range(args.warmup):
+        cpu_baseline(args)
+    vals, secs = [], 0.0
+    cb = None
+    for _ in range(args.steps):
+        cb = cpu_baseline(args)
+        vals.append(cb["value"])
+        secs += cb["seconds"]
+    v = statistics.median(vals)
+    cb["value"] = v
+    line.update({"value": v, "ms_per_step": round(secs / args.steps * 1e3, 3),
+                 "config": workload_config(args, world, note="CPU port of the reference algorithm, bounded sample"),
+                 "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                             "d2h_bytes_per_step": 0}})
+    return line
+
+
+def workload_config(args, world, note=None):
+    cap = 1 << args.cap_log
+    n = int(args.lf * cap)
+    d = {"workload": f"bulk insert of {n:,} unique uint32 keys into 2^{args.cap_log} slots (LF {args.lf}) then "
+                     f"{n:,} lookups ({args.present:.0%} present), {args.policy}",
+         "capacity_slots": cap, "keys_per_gpu": n, "lookups_per_gpu": n, "present_fraction": args.present,
+         "policy": args.policy, "seed": args.seed,
+         "l2": "inputs larger than L2 (table 512 MiB, each key array 241 MB); no flush",
+         "parallelism": f"replicas: {world} independent table(s), one per GPU"}
+    if note:
+        d["note"] = note
+    return d
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import torch
+    import torch.distributed as dist
+
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line:
+            print(json.dumps(line), flush=True)
+        return
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    import numpy as np
+    from hivehashtable_b200 import HiveHashTable, as_device_u32
+    from hivehashtable_b200 import workload
+
+    cap = 1 << args.cap_log
+    n = int(args.lf * cap)
+    keys_h, vals_h, look_h = workload.bulk_workload(args.seed + 1000 * rank, n, args.present)
+    n_look = look_h.size
+    keys = as_device_u32(keys_h, dev)
+    vals = as_device_u32(vals_h, dev)
+    look = as_device_u32(look_h, dev)
+    status = torch.empty(n, dtype=torch.uint8, device=dev)
+    fvals = torch.empty(n_look, dtype=torch.int32, device=dev)
+    found = torch.empty(n_look, dtype=torch.uint8, device=dev)
+    table = HiveHashTable(cap, args.policy)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(ev=None):
+        table.clear()
+        if ev:
+            ev[0].record(stream)
+        table.insert(keys, vals, status)
+        if ev:
+            ev[1].record(stream)
+        table.find(look, fvals, found)
+        if ev:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # correctness guard on the measured configuration: every insert placed, present keys found
+    st = status.cpu().numpy()
+    fnd = found.cpu().numpy()
+    n_present = int(round(n_look * args.present))
+    placed = int((st != 0).sum())
+    assert placed == n and int(fnd.sum()) == n_present, (placed, n, int(fnd.sum()), n_present)
+    table.check()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    with sampler:
+        t0.record(stream)
+        for i in range(args.steps):
+            step(evs[i])
+        t1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    ins_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    find_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    if world > 1:
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+
+    # end to end through the public API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        kh = torch.from_numpy(keys_h.view(np.int32)).pin_memory()
+        vh = torch.from_numpy(vals_h.view(np.int32)).pin_memory()
+        lh = torch.from_numpy(look_h.view(np.int32)).pin_memory()
+        st_h = torch.empty(n, dtype=torch.uint8).pin_memory()
+        fv_h = torch.empty(n_look, dtype=torch.int32).pin_memory()
+        fd_h = torch.empty(n_look, dtype=torch.uint8).pin_memory()
+        dk = torch.empty_like(keys)
+        dv = torch.empty_like(vals)
+        dl = torch.empty_like(look)
+
+        def e2e_step():
+            table.clear()
+            dk.copy_(kh, non_blocking=True)
+            dv.copy_(vh, non_blocking=True)
+            table.insert(dk, dv, status)
+            st_h.copy_(status, non_blocking=True)
+            dl.copy_(lh, non_blocking=True)
+            table.find(dl, fvals, found)
+            fv_h.copy_(fvals, non_blocking=True)
+            fd_h.copy_(found, non_blocking=True)
+
+        for _ in range(args.warmup):
+            e2e_step()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ems = a.elapsed_time(b)
+        if world > 1:
+            tt = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        assert int(fd_h.sum()) == n_present
+        e2e = {"value": round(2 * n * args.steps * world / (ems / 1e3) / 1e6, 2), "unit": UNIT,
+               "h2d_bytes_per_step": int(n * 8 + n_look * 4), "d2h_bytes_per_step": int(n + n_look * 5),
+               "ms_per_step": round(ems / args.steps, 4)}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_baseline(args)
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        ins_avg = sum(ins_ms) / len(ins_ms)
+        find_avg = sum(find_ms) / len(find_ms)
+        lb = n_present * BYTES_LOOKUP_PRESENT + (n_look - n_present) * BYTES_LOOKUP_ABSENT
+        kernels = {
+            "k_insert": {"ms": ins_avg, "bytes": n * BYTES_INSERT, "ops": n, "traffic_per_op": TRAFFIC_PER_OP["insert"]},
+            "k_find": {"ms": find_avg, "bytes": lb, "ops": n_look, "traffic_per_op": TRAFFIC_PER_OP["lookup"]},
+        }
+        rl = {}
+        for name, kd in kernels.items():
+            ach = kd["bytes"] / (kd["ms"] / 1e3) / 1e9
+            tr = kd["traffic_per_op"] * kd["ops"] if kd["traffic_per_op"] else None
+            rl[name] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(ach / peak, 4), "traffic": tr, "peak_kind": peak_kind,
+                        "algorithmic_bytes": kd["bytes"], "ms_per_launch": round(kd["ms"], 4),
+                        "mops": round(kd["ops"] / kd["ms"] / 1e3, 1)}
+        dom = max(kernels, key=lambda k: kernels[k]["ms"])
+        roof = dict(rl[dom], kernel=dom)
+        line = {"metric": METRIC, "value": round(2 * n * args.steps * world / (ms / 1e3) / 1e6, 2), "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seeded uint32 keys/values)",
+                "config": workload_config(args, world), "roofline": roof, "roofline_all": rl,
+                "insert_mops": rl["k_insert"]["mops"], "lookup_mops": rl["k_find"]["mops"],
+                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": 3 * args.steps,
+                "clocks": sampler.summary()}
+        print(json.dumps(line), flush=True)
+    table.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

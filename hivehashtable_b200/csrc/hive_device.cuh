@@ -1,0 +1,616 @@
+// hive_device.cuh -- device-side data layout, hash policies and per-operation protocols of the
+// B200 Hive hash table.  Included only by hive_table.cu.
+//
+// Layout in HBM (one table):
+//   slots      u64[nb_cap * 8]   8-slot buckets, 64 B each, 64 B aligned (the reference pads a
+//                                bucket to 128 B, include/hive_hash_table_struct.cuh:56-59; here
+//                                a bucket is exactly two 32 B sectors and one 256-bit load pair)
+//   stash      u64[nb_cap * 8]   per-canonical-bucket overflow stash, 8 slots
+//                                (include/hive_stash_table.cuh:20-27)
+//   stash_bits u32[nb_cap / 32]  bit b set = stash of bucket b may hold entries (the reference
+//                                keeps this as bit 31 of a per-bucket freeMask word,
+//                                include/hive_hash_insert.cuh:512-514); 1 bit per bucket keeps
+//                                it L2-resident (1 MiB at 2^23 buckets)
+//   lock_bits  u32[nb_cap / 32]  eviction locks, 1 bit per bucket (the reference uses a u32
+//                                word per bucket, include/hive_hash_table_struct.cuh:101-117)
+//   counters   u64[16]           slow-path event counters and the sticky error word
+//
+// A slot holds (value << 32) | key (include/hive_hash_table_struct.cuh:297-311); key 0 is the
+// empty sentinel, so an all-zero slot is free (include/utils.h:39-47).  There is no freeMask
+// array: a slot is free iff it reads 0, and a free slot is claimed with one 64-bit CAS.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hive {
+
+typedef unsigned long long u64;
+
+constexpr int kSlots = 8;
+
+// Per-op status codes (uint8 outputs).  Success is any non-zero code except kStError.
+enum : uint8_t {
+    kStFail = 0,      // insert: not placed (stash full) or key 0; find/erase: not found
+    kStInserted = 1,  // insert placed a new key in a bucket; find/erase/increment: success
+    kStUpdated = 2,   // insert overwrote the value of an existing key (upsert)
+    kStStashed = 3,   // insert placed a new key in the overflow stash
+    kStError = 0xFF,  // a bounded wait expired (lock timeout or retry budget spent)
+};
+
+// Counter slots.
+enum {
+    kCtrSlowPath = 0,     // inserts that found their canonical bucket full
+    kCtrEvictions = 1,    // victims moved H0 -> H1
+    kCtrStashPush = 2,    // keys written to the stash
+    kCtrFailed = 3,       // inserts that could not be placed
+    kCtrLockTimeout = 4,  // lock waits that expired
+    kCtrRetryOut = 5,     // CAS retry budgets that ran out
+    kCtrDupFixed = 6,     // duplicate copies removed after racing same-key inserts
+    kCtrError = 15,       // sticky error bits (kErr*)
+};
+enum : unsigned long long { kErrLockTimeout = 1ull, kErrRetryOut = 2ull };
+
+constexpr uint32_t kFlagHoles = 1u;  // deletes or a resize ran since the last clear
+
+// The device view of a table, passed to every kernel by value.
+//
+// Addressing is linear hashing over the policy's 32-bit hash h (level L, base N0):
+//   n_lo = N0 << L;  b = h mod n_lo;  if b < split: b = h mod 2*n_lo.
+// With L = 0 and split = 0 this is exactly the reference's get_bucket = hash % num_buckets
+// (include/HashPolicies.cuh:13-16).  Splitting bucket b moves its keys to b or b + n_lo.
+struct Table {
+    u64* slots;
+    u64* stash;
+    uint32_t* stash_bits;
+    uint32_t* lock_bits;
+    u64* counters;
+    u64 m_lo;  // fastmod magic for n_lo
+    u64 m_hi;  // fastmod magic for 2 * n_lo
+    uint32_t n_lo;
+    uint32_t split;
+    uint32_t max_evictions;
+    uint32_t flags;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Hashes (restated from include/hash.hpp of the reference; published integer hashes)
+// ---------------------------------------------------------------------------------------------
+
+// Thomas Wang's integer hash, the reference's hash1 (include/hash.hpp:29-37).
+__host__ __device__ __forceinline__ uint32_t wang_hash(uint32_t k) {
+    k = ~k + (k << 15);
+    k ^= k >> 12;
+    k += k << 2;
+    k ^= k >> 4;
+    k *= 2057u;
+    k ^= k >> 16;
+    return k;
+}
+
+// Bob Jenkins' 32-bit integer hash, the reference's hash2 (include/hash.hpp:49-62; its two PTX
+// lop3 0x96 steps are 3-input XORs).
+__host__ __device__ __forceinline__ uint32_t jenkins_hash(uint32_t k) {
+    k = (k + 0x7ed55d16u) + (k << 12);
+    k = (k ^ 0xc761c23cu) ^ (k >> 19);
+    k = (k + 0x165667b1u) + (k << 5);
+    k = (k + 0xd3a2646cu) ^ (k << 9);
+    k = (k + 0xfd7046c5u) + (k << 3);
+    k = (k ^ 0xb55a4f09u) ^ (k >> 16);
+    return k;
+}
+
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// One-block MurmurHash3_x86_32, seed 0, length 4: the reference's murmurhash
+// (include/hash.hpp:110-138).
+__host__ __device__ __forceinline__ uint32_t murmur_hash(uint32_t key) {
+    uint32_t k = key * 0xcc9e2d51u;
+    k = (k << 15) | (k >> 17);
+    k *= 0x1b873593u;
+    uint32_t h = (k << 13) | (k >> 19);
+    h = h * 5u + 0xe6546b64u;
+    return fmix32(h ^ 4u);
+}
+
+// The reference's cityhash mixer (include/hash.hpp:80-108).
+__host__ __device__ __forceinline__ uint32_t city_hash(uint32_t key) {
+    uint32_t k = key ^ 0x9ae16a3bu;
+    k *= 0xc2b2ae35u;
+    k ^= 0x1b873593u;
+    k *= 0x85ebca6bu;
+    uint32_t h = k * 0xc2b2ae35u;
+    h ^= 0x1b873593u;
+    h *= 0x85ebca6bu;
+    return fmix32(h ^ 4u);
+}
+
+// Hash policies: NumHashes = 2 and the two raw hashes of a key
+// (include/HashPolicies.cuh:10-17 Default2HashPolicy, :29-36 MurmurCityHashPolicy).
+template <int P>
+struct Policy;
+template <>
+struct Policy<0> {
+    __device__ __forceinline__ static uint32_t h0(uint32_t k) { return wang_hash(k); }
+    __device__ __forceinline__ static uint32_t h1(uint32_t k) { return jenkins_hash(k); }
+};
+template <>
+struct Policy<1> {
+    __device__ __forceinline__ static uint32_t h0(uint32_t k) { return murmur_hash(k); }
+    __device__ __forceinline__ static uint32_t h1(uint32_t k) { return city_hash(k); }
+};
+
+// a mod d for 32-bit a and d >= 1 with m = floor((2^64 - 1) / d) + 1 (Lemire, Kaser, Kurz,
+// "Faster Remainder by Direct Computation", 2019): exact for every 32-bit a and d.
+__device__ __forceinline__ uint32_t fastmod(uint32_t a, u64 m, uint32_t d) {
+    return (uint32_t)__umul64hi(m * (u64)a, (u64)d);
+}
+
+__device__ __forceinline__ uint32_t bucket_addr(const Table& t, uint32_t h) {
+    uint32_t b = fastmod(h, t.m_lo, t.n_lo);
+    if (b < t.split) b = fastmod(h, t.m_hi, t.n_lo << 1);
+    return b;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Bucket access
+// ---------------------------------------------------------------------------------------------
+
+struct Bucket {
+    u64 s[kSlots];
+};
+
+// Read-only kernels: the table does not change during the launch, so the non-coherent path is
+// valid; L1 allocation is skipped because bucket reads are random.
+__device__ __forceinline__ void load_bucket_ro(const u64* p, Bucket& b) {
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(b.s[0]), "=l"(b.s[1]), "=l"(b.s[2]), "=l"(b.s[3])
+                 : "l"(p));
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(b.s[4]), "=l"(b.s[5]), "=l"(b.s[6]), "=l"(b.s[7])
+                 : "l"(p + 4));
+}
+
+// Kernels that modify the table: relaxed gpu-scope loads are served by L2 (the coherence point),
+// never by a stale L1 line, so a retry after a lost CAS always sees the current bucket.
+__device__ __forceinline__ void load_bucket(const u64* p, Bucket& b) {
+    asm volatile("ld.relaxed.gpu.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(b.s[0]), "=l"(b.s[1]), "=l"(b.s[2]), "=l"(b.s[3])
+                 : "l"(p)
+                 : "memory");
+    asm volatile("ld.relaxed.gpu.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(b.s[4]), "=l"(b.s[5]), "=l"(b.s[6]), "=l"(b.s[7])
+                 : "l"(p + 4)
+                 : "memory");
+}
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ u64 pack(uint32_t k, uint32_t v) { return ((u64)v << 32) | k; }
+__device__ __forceinline__ uint32_t key_of(u64 kv) { return (uint32_t)kv; }
+__device__ __forceinline__ uint32_t val_of(u64 kv) { return (uint32_t)(kv >> 32); }
+
+// Bit j set: slot j holds key k (k != 0, so a match is never an empty slot).
+__device__ __forceinline__ uint32_t match_mask(const Bucket& b, uint32_t k) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j) m |= (uint32_t)(key_of(b.s[j]) == k) << j;
+    return m;
+}
+__device__ __forceinline__ uint32_t empty_mask(const Bucket& b) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j) m |= (uint32_t)(b.s[j] == 0ull) << j;
+    return m;
+}
+__device__ __forceinline__ u64 slot_at(const Bucket& b, int j) {
+    u64 r = b.s[0];
+#pragma unroll
+    for (int q = 1; q < kSlots; ++q)
+        if (q == j) r = b.s[q];
+    return r;
+}
+
+__device__ __forceinline__ u64 cas64(u64* p, u64 expect, u64 desired) {
+    return atomicCAS(p, expect, desired);
+}
+
+__device__ __forceinline__ bool stash_flag(const Table& t, uint32_t b) {
+    return (ld_relaxed_u32(t.stash_bits + (b >> 5)) >> (b & 31)) & 1u;
+}
+__device__ __forceinline__ bool stash_flag_ro(const Table& t, uint32_t b) {
+    return (__ldg(t.stash_bits + (b >> 5)) >> (b & 31)) & 1u;
+}
+
+__device__ __forceinline__ void count(const Table& t, int ctr) { atomicAdd(t.counters + ctr, 1ull); }
+__device__ __forceinline__ void raise_error(const Table& t, u64 bits) { atomicOr(t.counters + kCtrError, bits); }
+
+constexpr int kRetryLimit = 64;       // CAS retries of one op on one bucket
+constexpr int kLockSpinLimit = 1 << 16;  // lock attempts before the wait is declared expired
+
+// Bounded test-and-set on the bucket's lock bit.  Returns false when the wait expired.
+__device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
+    uint32_t* w = t.lock_bits + (b >> 5);
+    const uint32_t bit = 1u << (b & 31);
+    unsigned ns = 32;
+    for (int i = 0; i < kLockSpinLimit; ++i) {
+        if (!(atomicOr(w, bit) & bit)) {
+            __threadfence();
+            return true;
+        }
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+    }
+    count(t, kCtrLockTimeout);
+    raise_error(t, kErrLockTimeout);
+    return false;
+}
+__device__ __forceinline__ void unlock_bucket(const Table& t, uint32_t b) {
+    __threadfence();
+    atomicAnd(t.lock_bits + (b >> 5), ~(1u << (b & 31)));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Lookup: H0, H1, then the canonical stash gated by its flag
+// (include/hive_hash_lookup.cuh:126-155)
+// ---------------------------------------------------------------------------------------------
+
+template <int P, bool kReadOnly>
+__device__ __forceinline__ bool find_one(const Table& t, uint32_t k, uint32_t* v) {
+    if (k == 0) return false;
+    const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
+    Bucket B;
+    if (kReadOnly) load_bucket_ro(t.slots + (size_t)b0 * kSlots, B);
+    else load_bucket(t.slots + (size_t)b0 * kSlots, B);
+    uint32_t m = match_mask(B, k);
+    if (!m) {
+        const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
+        if (b1 != b0) {
+            if (kReadOnly) load_bucket_ro(t.slots + (size_t)b1 * kSlots, B);
+            else load_bucket(t.slots + (size_t)b1 * kSlots, B);
+            m = match_mask(B, k);
+        }
+        if (!m && (kReadOnly ? stash_flag_ro(t, b0) : stash_flag(t, b0))) {
+            if (kReadOnly) load_bucket_ro(t.stash + (size_t)b0 * kSlots, B);
+            else load_bucket(t.stash + (size_t)b0 * kSlots, B);
+            m = match_mask(B, k);
+        }
+        if (!m) return false;
+    }
+    *v = val_of(slot_at(B, __ffs(m) - 1));
+    return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Update in place: CAS the first copy of k in bucket p to kv.
+// Returns 1 updated, 0 key absent, -1 lost a race (caller reloads).
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ int update_in(u64* p, uint32_t k, u64 kv) {
+    Bucket B;
+    load_bucket(p, B);
+    uint32_t m = match_mask(B, k);
+    if (!m) return 0;
+    int j = __ffs(m) - 1;
+    u64 old = slot_at(B, j);
+    return cas64(p + j, old, kv) == old ? 1 : -1;
+}
+
+// Increment the value of the first copy of k in bucket p.  Returns 1 done (new value in *nv),
+// 0 absent, -1 lost a race.
+__device__ __forceinline__ int increment_in(u64* p, uint32_t k, uint32_t* nv) {
+    Bucket B;
+    load_bucket(p, B);
+    uint32_t m = match_mask(B, k);
+    if (!m) return 0;
+    int j = __ffs(m) - 1;
+    u64 old = slot_at(B, j);
+    uint32_t v = val_of(old) + 1u;
+    if (cas64(p + j, old, pack(k, v)) != old) return -1;
+    *nv = v;
+    return 1;
+}
+
+// After claiming slot j of bucket p for k while deletes may run (kFlagHoles), two inserts of the
+// same key can claim different slots.  Keep the lower-indexed copy; whichever of the two racing
+// inserts sees the other removes the higher one (a CAS from the exact value, so at most one
+// removal happens and nothing else is ever removed).  Returns true if this op's own copy was
+// the one removed.
+__device__ __forceinline__ bool resolve_duplicate(const Table& t, u64* p, uint32_t k, int j, u64 kv) {
+    __threadfence();
+    Bucket B;
+    load_bucket(p, B);
+    uint32_t m = match_mask(B, k) & ~(1u << j);
+    if (!m) return false;
+    int o = __ffs(m) - 1;
+    if (o < j) {
+        if (cas64(p + j, kv, 0ull) == kv) {
+            count(t, kCtrDupFixed);
+            return true;
+        }
+        return false;
+    }
+    u64 theirs = slot_at(B, o);
+    if (cas64(p + o, theirs, 0ull) == theirs) count(t, kCtrDupFixed);
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Insert = upsert (S2).  Four stages as in include/hive_hash_insert.cuh:898-1042:
+//   A  try-replace in the candidate buckets and the canonical stash,
+//   B  claim a free slot of the canonical bucket H0 with a 64-bit CAS,
+//   C  bounded depth-1 cuckoo eviction from H0 under H0's lock,
+//   D  the canonical bucket's overflow stash.
+//
+// Invariants that keep every key in exactly one place and visible at all times:
+//   * a new key is only ever placed in its canonical bucket H0 (or H0's stash);
+//   * a victim is moved only from its own H0 to its H1, and is written to H1 before its H0 slot
+//     is overwritten, so a reader scanning H0 then H1 always sees it;
+//   * an evictor holds H0's lock, so one victim has one mover;
+//   * every slot change is a CAS from an observed value, so a concurrent update or delete of
+//     the victim is detected and either propagated to the copy or undone.
+// Without kFlagHoles (no delete or resize since the last clear) slots only ever go from free to
+// occupied, so a key can live in H1 or in the stash only if H0 is full: stage B may then claim in
+// H0 without reading H1 first, and two inserts of one key always race for the same lowest free
+// slot (so they cannot both succeed).
+// ---------------------------------------------------------------------------------------------
+
+enum { kEvPlaced = 1, kEvRetry = 2, kEvNone = 0 };
+
+template <int P>
+__device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket& B0, uint32_t b0, u64 kv) {
+    const int limit = t.max_evictions < (uint32_t)kSlots ? (int)t.max_evictions : kSlots;
+    for (int j = 0; j < limit; ++j) {
+        u64 vkv = slot_at(B0, j);
+        if (vkv == 0ull) {
+            // A slot freed up (delete) since the bucket was read.
+            return cas64(B0p + j, 0ull, kv) == 0ull ? kEvPlaced : kEvRetry;
+        }
+        const uint32_t vk = key_of(vkv);
+        if (bucket_addr(t, Policy<P>::h0(vk)) != b0) continue;  // victim lives in its H1
+        const uint32_t alt = bucket_addr(t, Policy<P>::h1(vk));
+        if (alt == b0) continue;
+        u64* Ap = t.slots + (size_t)alt * kSlots;
+        Bucket A;
+        load_bucket(Ap, A);
+        uint32_t e = empty_mask(A);
+        if (!e) continue;
+        const int d = __ffs(e) - 1;
+        if (cas64(Ap + d, 0ull, vkv) != 0ull) continue;  // lost the free slot; next victim
+        // The victim is now visible in both H0 slot j and H1 slot d.
+        for (int r = 0; r < kRetryLimit; ++r) {
+            u64 obs = cas64(B0p + j, vkv, kv);
+            if (obs == vkv) {
+                count(t, kCtrEvictions);
+                return kEvPlaced;
+            }
+            if (obs == 0ull) {
+                // Victim deleted meanwhile: drop the copy unless it changed, take the free slot.
+                cas64(Ap + d, vkv, 0ull);
+                return cas64(B0p + j, 0ull, kv) == 0ull ? kEvPlaced : kEvRetry;
+            }
+            if (key_of(obs) == vk) {
+                // Victim updated meanwhile: carry the new value to the copy, then retry.
+                if (cas64(Ap + d, vkv, obs) != vkv) return kEvRetry;
+                vkv = obs;
+                continue;
+            }
+            cas64(Ap + d, vkv, 0ull);
+            return kEvRetry;
+        }
+        count(t, kCtrRetryOut);
+        raise_error(t, kErrRetryOut);
+        return kEvRetry;
+    }
+    return kEvNone;
+}
+
+// Stage C/D under H0's lock.  The caller holds the lock on b0.
+template <int P>
+__device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
+    u64* B0p = t.slots + (size_t)b0 * kSlots;
+    u64* B1p = t.slots + (size_t)b1 * kSlots;
+    u64* Sp = t.stash + (size_t)b0 * kSlots;
+    const bool holes = t.flags & kFlagHoles;
+    for (int r = 0; r < kRetryLimit; ++r) {
+        Bucket B0, B1;
+        load_bucket(B0p, B0);
+        load_bucket(B1p, B1);
+        uint32_t m = match_mask(B0, k);
+        if (m) {
+            int j = __ffs(m) - 1;
+            u64 old = slot_at(B0, j);
+            if (cas64(B0p + j, old, kv) == old) return kStUpdated;
+            continue;
+        }
+        m = match_mask(B1, k);
+        if (m) {
+            int j = __ffs(m) - 1;
+            u64 old = slot_at(B1, j);
+            if (cas64(B1p + j, old, kv) == old) return kStUpdated;
+            continue;
+        }
+        if (stash_flag(t, b0)) {
+            int u = update_in(Sp, k, kv);
+            if (u == 1) return kStUpdated;
+            if (u < 0) continue;
+        }
+        uint32_t e = empty_mask(B0);
+        if (e) {
+            int j = __ffs(e) - 1;
+            if (cas64(B0p + j, 0ull, kv) == 0ull) {
+                if (holes && resolve_duplicate(t, B0p, k, j, kv)) return kStUpdated;
+                return kStInserted;
+            }
+            continue;
+        }
+        int ev = try_evict<P>(t, B0p, B0, b0, kv);
+        if (ev == kEvPlaced) return kStInserted;
+        if (ev == kEvRetry) continue;
+        // Stage D: the canonical bucket's stash.  Its flag is raised before the entry is
+        // written, so a reader that finds the entry also finds the flag set.
+        atomicOr(t.stash_bits + (b0 >> 5), 1u << (b0 & 31));
+        __threadfence();
+        for (int q = 0; q < kRetryLimit; ++q) {
+            Bucket S;
+            load_bucket(Sp, S);
+            uint32_t se = empty_mask(S);
+            if (!se) {
+                count(t, kCtrFailed);
+                return kStFail;
+            }
+            int j = __ffs(se) - 1;
+            if (cas64(Sp + j, 0ull, kv) == 0ull) {
+                count(t, kCtrStashPush);
+                return kStStashed;
+            }
+        }
+        break;
+    }
+    count(t, kCtrRetryOut);
+    raise_error(t, kErrRetryOut);
+    return kStError;
+}
+
+template <int P>
+__device__ __noinline__ uint8_t insert_slow(const Table& t, uint32_t k, u64 kv, uint32_t b0) {
+    const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
+    const bool holes = t.flags & kFlagHoles;
+    u64* B0p = t.slots + (size_t)b0 * kSlots;
+    u64* B1p = t.slots + (size_t)b1 * kSlots;
+    u64* Sp = t.stash + (size_t)b0 * kSlots;
+    count(t, kCtrSlowPath);
+    // Lock-free stage A over H1 and the stash; with holes also stage B in H0.
+    for (int r = 0; r < kRetryLimit; ++r) {
+        int u = update_in(B0p, k, kv);
+        if (u == 1) return kStUpdated;
+        if (u < 0) continue;
+        if (b1 != b0) {
+            u = update_in(B1p, k, kv);
+            if (u == 1) return kStUpdated;
+            if (u < 0) continue;
+        }
+        if (stash_flag(t, b0)) {
+            u = update_in(Sp, k, kv);
+            if (u == 1) return kStUpdated;
+            if (u < 0) continue;
+        }
+        if (holes) {
+            Bucket B0;
+            load_bucket(B0p, B0);
+            uint32_t e = empty_mask(B0);
+            if (match_mask(B0, k)) continue;
+            if (e) {
+                int j = __ffs(e) - 1;
+                if (cas64(B0p + j, 0ull, kv) == 0ull) {
+                    if (resolve_duplicate(t, B0p, k, j, kv)) return kStUpdated;
+                    return kStInserted;
+                }
+                continue;
+            }
+        }
+        break;
+    }
+    if (!lock_bucket(t, b0)) return kStError;
+    uint8_t st = insert_locked<P>(t, k, kv, b0, b1);
+    unlock_bucket(t, b0);
+    return st;
+}
+
+template <int P>
+__device__ __forceinline__ uint8_t insert_one(const Table& t, uint32_t k, uint32_t v) {
+    if (k == 0) return kStFail;
+    const u64 kv = pack(k, v);
+    const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
+    if (!(t.flags & kFlagHoles)) {
+        u64* B0p = t.slots + (size_t)b0 * kSlots;
+        for (int r = 0; r < kRetryLimit; ++r) {
+            Bucket B;
+            load_bucket(B0p, B);
+            uint32_t m = match_mask(B, k);
+            if (m) {
+                int j = __ffs(m) - 1;
+                u64 old = slot_at(B, j);
+                if (cas64(B0p + j, old, kv) == old) return kStUpdated;
+                continue;
+            }
+            uint32_t e = empty_mask(B);
+            if (!e) break;
+            if (cas64(B0p + (__ffs(e) - 1), 0ull, kv) == 0ull) return kStInserted;
+        }
+    }
+    return insert_slow<P>(t, k, kv, b0);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Delete: remove every copy in H0, H1 and the canonical stash, no early exit
+// (include/hive_hash_delete.cuh:168-194).  Returns true if any copy was removed.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool erase_in(const Table& t, u64* p, uint32_t k) {
+    bool removed = false;
+    for (int r = 0; r < kRetryLimit; ++r) {
+        Bucket B;
+        load_bucket(p, B);
+        uint32_t m = match_mask(B, k);
+        if (!m) return removed;
+        int j = __ffs(m) - 1;
+        u64 old = slot_at(B, j);
+        if (cas64(p + j, old, 0ull) == old) removed = true;
+    }
+    count(t, kCtrRetryOut);
+    raise_error(t, kErrRetryOut);
+    return removed;
+}
+
+template <int P>
+__device__ __forceinline__ bool erase_one(const Table& t, uint32_t k) {
+    if (k == 0) return false;
+    const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
+    const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
+    bool removed = erase_in(t, t.slots + (size_t)b0 * kSlots, k);
+    if (b1 != b0) removed |= erase_in(t, t.slots + (size_t)b1 * kSlots, k);
+    if (stash_flag(t, b0)) removed |= erase_in(t, t.stash + (size_t)b0 * kSlots, k);
+    return removed;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Increment (the reference's OperationType::ATOMIC_INC, include/utils.h:14, which its mixed
+// kernel leaves unhandled): value += 1 on the first copy found in H0, H1, stash order.
+// ---------------------------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ bool increment_one(const Table& t, uint32_t k, uint32_t* nv) {
+    if (k == 0) return false;
+    const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
+    const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
+    for (int r = 0; r < kRetryLimit; ++r) {
+        int u = increment_in(t.slots + (size_t)b0 * kSlots, k, nv);
+        if (u == 1) return true;
+        if (u < 0) continue;
+        if (b1 != b0) {
+            u = increment_in(t.slots + (size_t)b1 * kSlots, k, nv);
+            if (u == 1) return true;
+            if (u < 0) continue;
+        }
+        if (stash_flag(t, b0)) {
+            u = increment_in(t.stash + (size_t)b0 * kSlots, k, nv);
+            if (u == 1) return true;
+            if (u < 0) continue;
+        }
+        return false;
+    }
+    count(t, kCtrRetryOut);
+    raise_error(t, kErrRetryOut);
+    return false;
+}
+
+}  // namespace hive

@@ -1,0 +1,773 @@
+// hive_table.cu -- kernels and the C ABI (include/hive_c.h) of the B200 Hive hash table.
+//
+// One thread owns one operation: it loads a whole 64 B bucket with two 256-bit loads, matches
+// all 8 slots in registers and commits with one 64-bit CAS, so a warp keeps 32 independent
+// random bucket reads in flight (the reference serialises 4 ops per 4-lane tile,
+// include/hive_kernels.cuh:205-266).  Grids are one thread per op in 256-thread blocks.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "hive_c.h"
+#include "hive_device.cuh"
+
+using hive::u64;
+
+namespace {
+
+thread_local int g_last_cuda_error = 0;
+
+constexpr int kBlock = 256;
+constexpr double kMaxShrinkLoad = 0.9;
+
+inline int cuda_fail(cudaError_t e) {
+    g_last_cuda_error = (int)e;
+    return e == cudaErrorMemoryAllocation ? HIVE_ERR_OOM : HIVE_ERR_CUDA;
+}
+
+#define HIVE_CUDA(call)                              \
+    do {                                             \
+        cudaError_t e_ = (call);                     \
+        if (e_ != cudaSuccess) return cuda_fail(e_); \
+    } while (0)
+
+inline u64 fastmod_magic(uint32_t d) { return ~0ull / (u64)d + 1ull; }
+
+inline unsigned grid_for(uint64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+// Keeps the table's device current for the duration of a call and restores the caller's.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) { ok = false; return; }
+        if (prev != dev && cudaSetDevice(dev) != cudaSuccess) ok = false;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct hive_table {
+    int device = 0;
+    int policy = 0;
+    hive::Table t{};
+    uint64_t nb_cap = 0;     // buckets allocated
+    uint32_t n0 = 0;         // level-0 bucket count
+    uint32_t level = 0;
+    void* block = nullptr;   // single allocation holding every array
+    size_t block_bytes = 0;
+    u64* scratch = nullptr;  // 8-byte device scratch for size/dump counts
+};
+
+namespace {
+
+inline uint64_t num_buckets(const hive_table* h) { return (uint64_t)h->t.n_lo + h->t.split; }
+
+void set_geometry(hive_table* h, uint32_t level, uint32_t split) {
+    h->level = level;
+    h->t.n_lo = h->n0 << level;
+    h->t.split = split;
+    h->t.m_lo = fastmod_magic(h->t.n_lo);
+    h->t.m_hi = fastmod_magic(h->t.n_lo << 1);
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct Carve {
+    size_t slots, stash, sbits, lbits, ctr, scratch, total;
+};
+Carve carve(uint64_t nb_cap) {
+    Carve c;
+    size_t words = (size_t)((nb_cap + 31) / 32);
+    c.slots = 0;
+    c.stash = align256(c.slots + (size_t)nb_cap * 64);
+    c.sbits = align256(c.stash + (size_t)nb_cap * 64);
+    c.lbits = align256(c.sbits + words * 4);
+    c.ctr = align256(c.lbits + words * 4);
+    c.scratch = align256(c.ctr + HIVE_NUM_COUNTERS * 8);
+    c.total = align256(c.scratch + 8);
+    return c;
+}
+
+void bind_arrays(hive_table* h, void* block, uint64_t nb_cap) {
+    Carve c = carve(nb_cap);
+    char* base = (char*)block;
+    h->block = block;
+    h->block_bytes = c.total;
+    h->nb_cap = nb_cap;
+    h->t.slots = (u64*)(base + c.slots);
+    h->t.stash = (u64*)(base + c.stash);
+    h->t.stash_bits = (uint32_t*)(base + c.sbits);
+    h->t.lock_bits = (uint32_t*)(base + c.lbits);
+    h->t.counters = (u64*)(base + c.ctr);
+    h->scratch = (u64*)(base + c.scratch);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------------------------
+
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_insert(hive::Table t, const uint32_t* __restrict__ keys,
+                                                   const uint32_t* __restrict__ vals, uint64_t n,
+                                                   uint8_t* __restrict__ status) {
+    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = __ldcs(keys + i);
+    const uint32_t v = __ldcs(vals + i);
+    const uint8_t st = hive::insert_one<P>(t, k, v);
+    if (status) __stcs(status + i, st);
+}
+
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_find(hive::Table t, const uint32_t* __restrict__ keys, uint64_t n,
+                                                 uint32_t* __restrict__ vals, uint8_t* __restrict__ found) {
+    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = __ldcs(keys + i);
+    uint32_t v = 0;
+    const bool f = hive::find_one<P, true>(t, k, &v);
+    if (vals) __stcs(vals + i, f ? v : 0u);
+    if (found) __stcs(found + i, (uint8_t)f);
+}
+
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_erase(hive::Table t, const uint32_t* __restrict__ keys, uint64_t n,
+                                                  uint8_t* __restrict__ status) {
+    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const bool r = hive::erase_one<P>(t, __ldcs(keys + i));
+    if (status) __stcs(status + i, (uint8_t)r);
+}
+
+template <int P>
+__device__ __forceinline__ uint8_t apply_one(const hive::Table& t, uint8_t type, uint32_t k, uint32_t v,
+                                             uint32_t* out) {
+    *out = 0;
+    switch (type) {
+        case HIVE_OP_INSERT:
+            return hive::insert_one<P>(t, k, v);
+        case HIVE_OP_LOOKUP: {
+            uint32_t fv = 0;
+            bool f = hive::find_one<P, false>(t, k, &fv);
+            *out = f ? fv : 0u;
+            return (uint8_t)f;
+        }
+        case HIVE_OP_DELETE:
+            return (uint8_t)hive::erase_one<P>(t, k);
+        case HIVE_OP_INCREMENT: {
+            uint32_t nv = 0;
+            bool f = hive::increment_one<P>(t, k, &nv);
+            *out = f ? nv : 0u;
+            return (uint8_t)f;
+        }
+        default:
+            return 0;
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_apply(hive::Table t, const uint8_t* __restrict__ types,
+                                                  const uint32_t* __restrict__ keys,
+                                                  const uint32_t* __restrict__ vals, uint64_t n,
+                                                  uint8_t* __restrict__ status, uint32_t* __restrict__ outv) {
+    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    uint32_t o;
+    const uint8_t st = apply_one<P>(t, __ldcs(types + i), __ldcs(keys + i), vals ? __ldcs(vals + i) : 0u, &o);
+    if (status) __stcs(status + i, st);
+    if (outv) __stcs(outv + i, o);
+}
+
+// Reference Operation records: {int32 type; pad; uint64 key} (include/utils.h:18-21).
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_apply_ref(hive::Table t, const ulonglong2* __restrict__ ops, uint64_t n,
+                                                      unsigned long long* __restrict__ results) {
+    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const ulonglong2 rec = __ldcs(ops + i);
+    const int32_t type = (int32_t)(uint32_t)rec.x;
+    const uint32_t k = (uint32_t)rec.y;
+    uint32_t o;
+    uint8_t st = (type >= 0 && type <= 3) ? apply_one<P>(t, (uint8_t)type, k, k + 1u, &o) : 0;
+    if (results) __stcs(results + i, (unsigned long long)(st != hive::kStFail && st != hive::kStError));
+}
+
+template <int P>
+__global__ void k_bucket_of(hive::Table t, const uint32_t* __restrict__ keys, uint64_t n, uint32_t* b0,
+                            uint32_t* b1) {
+    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = keys[i];
+    if (b0) b0[i] = hive::bucket_addr(t, hive::Policy<P>::h0(k));
+    if (b1) b1[i] = hive::bucket_addr(t, hive::Policy<P>::h1(k));
+}
+
+// Zero the stash buckets whose flag is set; one thread per flag word.
+__global__ void k_clear_stash(hive::Table t, uint64_t words) {
+    const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= words) return;
+    uint32_t bits = t.stash_bits[w];
+    while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        ulonglong4* p = reinterpret_cast<ulonglong4*>(t.stash + (w * 32 + b) * hive::kSlots);
+        p[0] = make_ulonglong4(0, 0, 0, 0);
+        p[1] = make_ulonglong4(0, 0, 0, 0);
+    }
+}
+
+__device__ __forceinline__ uint32_t occupied(const hive::Bucket& B) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < hive::kSlots; ++j) c += B.s[j] != 0ull;
+    return c;
+}
+
+// Live entries in buckets [0, nb) and their stashes; warp-reduced, one atomic per warp.
+__global__ void k_count(hive::Table t, uint64_t nb, u64* out) {
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c = 0;
+    if (b < nb) {
+        hive::Bucket B;
+        hive::load_bucket_ro(t.slots + b * hive::kSlots, B);
+        c = occupied(B);
+        if ((t.stash_bits[b >> 5] >> (b & 31)) & 1u) {
+            hive::load_bucket_ro(t.stash + b * hive::kSlots, B);
+            c += occupied(B);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (u64)c);
+}
+
+// Compacts every live entry into kv[0, cap); *cnt ends as the total.
+__global__ void k_dump(hive::Table t, uint64_t nb, u64* __restrict__ kv, uint64_t cap, u64* cnt) {
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    hive::Bucket B, S;
+    uint32_t c = 0;
+    bool st = false;
+    if (b < nb) {
+        hive::load_bucket_ro(t.slots + b * hive::kSlots, B);
+        c = occupied(B);
+        st = (t.stash_bits[b >> 5] >> (b & 31)) & 1u;
+        if (st) {
+            hive::load_bucket_ro(t.stash + b * hive::kSlots, S);
+            c += occupied(S);
+        }
+    }
+    const unsigned lane = threadIdx.x & 31;
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    u64 base = 0;
+    if (lane == 31 && total) base = atomicAdd(cnt, (u64)total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    u64 pos = base + incl - c;
+    if (b < nb) {
+#pragma unroll
+        for (int j = 0; j < hive::kSlots; ++j)
+            if (B.s[j]) {
+                if (pos < cap) kv[pos] = B.s[j];
+                ++pos;
+            }
+        if (st) {
+#pragma unroll
+            for (int j = 0; j < hive::kSlots; ++j)
+                if (S.s[j]) {
+                    if (pos < cap) kv[pos] = S.s[j];
+                    ++pos;
+                }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Resize: linear hashing.  Split moves the keys of buckets [s, s + cnt) that now address
+// b + n_lo; merge folds buckets [s - cnt + n_lo, s + n_lo) back into [s - cnt, s).  Both run
+// between other kernels on the stream, so each bucket pair has a single owner thread.
+// (The reference's host loop is include/hive_hash_resize.cuh:138-215 / :340-420; its kernels are
+// not reused because of the defects listed there: slots 4-7 never split, modulus = index_mask.)
+// ---------------------------------------------------------------------------------------------
+
+template <int P>
+__device__ __forceinline__ uint32_t resident_hash(const hive::Table& t, uint32_t k, uint32_t b, bool* via0) {
+    const uint32_t h0 = hive::Policy<P>::h0(k);
+    if (hive::bucket_addr(t, h0) == b) {
+        *via0 = true;
+        return h0;
+    }
+    *via0 = false;
+    return hive::Policy<P>::h1(k);
+}
+
+// told: geometry before the split (split = s); tnew: after (split = s + cnt).
+template <int P>
+__global__ void k_split(hive::Table told, hive::Table tnew, uint32_t s, uint32_t cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    const uint32_t b = s + i, nbk = b + told.n_lo;
+    u64* src = told.slots + (size_t)b * hive::kSlots;
+    u64* dst = told.slots + (size_t)nbk * hive::kSlots;
+    hive::Bucket B;
+    hive::load_bucket(src, B);
+    int nd = 0;
+    u64 keep[hive::kSlots];
+    int nk = 0;
+#pragma unroll
+    for (int j = 0; j < hive::kSlots; ++j) {
+        const u64 kv = B.s[j];
+        if (!kv) continue;
+        bool via0;
+        const uint32_t h = resident_hash<P>(told, hive::key_of(kv), b, &via0);
+        if (hive::bucket_addr(tnew, h) == nbk) dst[nd++] = kv;
+        else keep[nk++] = kv;
+    }
+    for (int j = 0; j < hive::kSlots; ++j) src[j] = j < nk ? keep[j] : 0ull;
+    // Stash entries of canonical bucket b: re-place them by their new canonical bucket, into a
+    // free slot when there is one, else into that bucket's stash.
+    if ((told.stash_bits[b >> 5] >> (b & 31)) & 1u) {
+        u64* sb = told.stash + (size_t)b * hive::kSlots;
+        u64* sn = told.stash + (size_t)nbk * hive::kSlots;
+        hive::Bucket S;
+        hive::load_bucket(sb, S);
+        int keep_s = 0, moved_s = 0;
+        u64 ks[hive::kSlots];
+        for (int j = 0; j < hive::kSlots; ++j) {
+            const u64 kv = S.s[j];
+            if (!kv) continue;
+            const uint32_t c = hive::bucket_addr(tnew, hive::Policy<P>::h0(hive::key_of(kv)));
+            if (c == b && nk < hive::kSlots) {
+                src[nk++] = kv;
+            } else if (c == nbk && nd < hive::kSlots) {
+                dst[nd++] = kv;
+            } else if (c == b) {
+                ks[keep_s++] = kv;
+            } else {
+                sn[moved_s++] = kv;
+            }
+        }
+        for (int j = 0; j < hive::kSlots; ++j) sb[j] = j < keep_s ? ks[j] : 0ull;
+        if (!keep_s) atomicAnd(told.stash_bits + (b >> 5), ~(1u << (b & 31)));
+        if (moved_s) atomicOr(told.stash_bits + (nbk >> 5), 1u << (nbk & 31));
+    }
+}
+
+// told: geometry before (buckets [lo, lo + cnt) + n_lo are folded); tnew: after.
+// Entries that find no room are appended to ovf for re-insertion.
+template <int P>
+__global__ void k_merge(hive::Table told, hive::Table tnew, uint32_t lo, uint32_t cnt, u64* ovf, u64* novf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    const uint32_t b = lo + i, src_b = b + told.n_lo;
+    u64* src = told.slots + (size_t)src_b * hive::kSlots;
+    u64* ss = told.stash + (size_t)src_b * hive::kSlots;
+    const bool has_stash = (told.stash_bits[src_b >> 5] >> (src_b & 31)) & 1u;
+    for (int part = 0; part < (has_stash ? 2 : 1); ++part) {
+        u64* from = part ? ss : src;
+        hive::Bucket B;
+        hive::load_bucket(from, B);
+        for (int j = 0; j < hive::kSlots; ++j) {
+            const u64 kv = B.s[j];
+            if (!kv) continue;
+            from[j] = 0ull;
+            // Under the new geometry every key of src_b addresses b through the same hash.
+            bool placed = false;
+            u64* dstp = tnew.slots + (size_t)b * hive::kSlots;
+            for (int q = 0; q < hive::kSlots && !placed; ++q)
+                if (hive::cas64(dstp + q, 0ull, kv) == 0ull) placed = true;
+            if (!placed) ovf[atomicAdd(novf, 1ull)] = kv;
+        }
+    }
+    if (has_stash) atomicAnd(told.stash_bits + (src_b >> 5), ~(1u << (src_b & 31)));
+}
+
+// Re-insert overflow entries produced by k_merge through the normal insert protocol.
+template <int P>
+__global__ void k_reinsert(hive::Table t, const u64* __restrict__ kv, const u64* __restrict__ n, uint8_t* fail) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *n) return;
+    const u64 e = kv[i];
+    const uint8_t st = hive::insert_one<P>(t, hive::key_of(e), hive::val_of(e));
+    if (st == hive::kStFail || st == hive::kStError) *fail = 1;
+}
+
+template <template <int> class K>
+struct ByPolicy;
+
+int launch_check() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e);
+    return HIVE_OK;
+}
+
+int reset(hive_table* h, cudaStream_t s) {
+    const uint64_t nb = num_buckets(h);
+    const uint64_t words = (h->nb_cap + 31) / 32;
+    HIVE_CUDA(cudaMemsetAsync(h->t.slots, 0, (size_t)nb * 64, s));
+    k_clear_stash<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(h->t, words);
+    int rc = launch_check();
+    if (rc) return rc;
+    HIVE_CUDA(cudaMemsetAsync(h->t.stash_bits, 0, (size_t)words * 4, s));
+    HIVE_CUDA(cudaMemsetAsync(h->t.lock_bits, 0, (size_t)words * 4, s));
+    HIVE_CUDA(cudaMemsetAsync(h->t.counters, 0, HIVE_NUM_COUNTERS * 8, s));
+    return HIVE_OK;
+}
+
+bool valid_table(const hive_table* h) { return h && h->block; }
+
+int grow_capacity(hive_table* h, uint64_t need_buckets, cudaStream_t s) {
+    if (need_buckets <= h->nb_cap) return HIVE_OK;
+    uint64_t nb_cap = std::max<uint64_t>(need_buckets, h->nb_cap * 2);
+    if (nb_cap > 0xFFFFFFFFull) nb_cap = 0xFFFFFFFFull;
+    if (need_buckets > nb_cap) return HIVE_ERR_CAPACITY;
+    Carve c = carve(nb_cap), oc = carve(h->nb_cap);
+    void* nblock = nullptr;
+    HIVE_CUDA(cudaStreamSynchronize(s));
+    cudaError_t e = cudaMalloc(&nblock, c.total);
+    if (e != cudaSuccess) return cuda_fail(e);
+    char *nbase = (char*)nblock, *obase = (char*)h->block;
+    const uint64_t nb = num_buckets(h);
+    const size_t owords = (size_t)((h->nb_cap + 31) / 32);
+    if ((e = cudaMemsetAsync(nblock, 0, c.total, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(nbase + c.slots, obase + oc.slots, (size_t)nb * 64, cudaMemcpyDeviceToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(nbase + c.stash, obase + oc.stash, (size_t)nb * 64, cudaMemcpyDeviceToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(nbase + c.sbits, obase + oc.sbits, owords * 4, cudaMemcpyDeviceToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(nbase + c.ctr, obase + oc.ctr, HIVE_NUM_COUNTERS * 8, cudaMemcpyDeviceToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        cudaFree(nblock);
+        return cuda_fail(e);
+    }
+    cudaFree(h->block);
+    bind_arrays(h, nblock, nb_cap);
+    return HIVE_OK;
+}
+
+template <int P>
+int split_range(hive_table* h, uint32_t cnt, cudaStream_t s) {
+    hive::Table told = h->t;
+    const uint32_t sp = h->t.split;
+    hive::Table tnew = told;
+    tnew.split = sp + cnt;
+    k_split<P><<<(cnt + 127) / 128, 128, 0, s>>>(told, tnew, sp, cnt);
+    int rc = launch_check();
+    if (rc) return rc;
+    if (sp + cnt == h->t.n_lo) set_geometry(h, h->level + 1, 0);
+    else set_geometry(h, h->level, sp + cnt);
+    return HIVE_OK;
+}
+
+template <int P>
+int merge_range(hive_table* h, uint32_t cnt, cudaStream_t s) {
+    // Fold buckets [split - cnt, split) + n_lo back into [split - cnt, split).
+    hive::Table told = h->t;
+    const uint32_t lo = h->t.split - cnt;
+    hive::Table tnew = told;
+    tnew.split = lo;
+    u64* ovf = nullptr;
+    const size_t ovf_cap = (size_t)cnt * 16 + 1;
+    HIVE_CUDA(cudaMallocAsync(&ovf, ovf_cap * 8 + 16, s));
+    u64* novf = ovf + ovf_cap;
+    uint8_t* fail = (uint8_t*)(novf + 1);
+    HIVE_CUDA(cudaMemsetAsync(novf, 0, 16, s));
+    k_merge<P><<<(cnt + 127) / 128, 128, 0, s>>>(told, tnew, lo, cnt, ovf, novf);
+    int rc = launch_check();
+    if (rc) return rc;
+    h->t.split = lo;
+    tnew.flags |= hive::kFlagHoles;
+    k_reinsert<P><<<(unsigned)((ovf_cap + 255) / 256), 256, 0, s>>>(tnew, ovf, novf, fail);
+    if ((rc = launch_check())) return rc;
+    uint8_t hfail = 0;
+    HIVE_CUDA(cudaMemcpyAsync(&hfail, fail, 1, cudaMemcpyDeviceToHost, s));
+    HIVE_CUDA(cudaFreeAsync(ovf, s));
+    HIVE_CUDA(cudaStreamSynchronize(s));
+    return hfail ? HIVE_ERR_CAPACITY : HIVE_OK;
+}
+
+template <int P>
+int resize_impl(hive_table* h, uint64_t target_buckets, cudaStream_t s) {
+    h->t.flags |= hive::kFlagHoles;
+    int rc = HIVE_OK;
+    while (num_buckets(h) < target_buckets) {
+        const uint64_t need = target_buckets - num_buckets(h);
+        const uint32_t cnt = (uint32_t)std::min<uint64_t>(need, h->t.n_lo - h->t.split);
+        if ((rc = split_range<P>(h, cnt, s))) return rc;
+    }
+    while (num_buckets(h) > target_buckets) {
+        if (h->t.split == 0) {
+            if (h->level == 0) break;
+            set_geometry(h, h->level - 1, h->t.n_lo >> 1);
+        }
+        const uint64_t extra = num_buckets(h) - target_buckets;
+        const uint32_t cnt = (uint32_t)std::min<uint64_t>(extra, h->t.split);
+        if ((rc = merge_range<P>(h, cnt, s))) return rc;
+    }
+    return HIVE_OK;
+}
+
+}  // namespace
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+
+extern "C" {
+
+const char* hive_strerror(int status) {
+    switch (status) {
+        case HIVE_OK: return "ok";
+        case HIVE_ERR_INVALID_ARG: return "invalid argument";
+        case HIVE_ERR_CUDA: return "CUDA runtime error";
+        case HIVE_ERR_OOM: return "device out of memory";
+        case HIVE_ERR_LOCK_TIMEOUT: return "bucket lock wait expired inside a kernel";
+        case HIVE_ERR_RETRY_LIMIT: return "CAS retry budget ran out inside a kernel";
+        case HIVE_ERR_CAPACITY: return "capacity exceeded";
+        case HIVE_ERR_NO_DEVICE: return "no usable CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int hive_last_cuda_error(void) { return g_last_cuda_error; }
+
+int hive_create(const hive_config* cfg, hive_table** out) {
+    if (!cfg || !out) return HIVE_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (cfg->policy != HIVE_POLICY_DEFAULT2HASH && cfg->policy != HIVE_POLICY_MURMURCITYHASH)
+        return HIVE_ERR_INVALID_ARG;
+    if (cfg->max_evictions < 0 || cfg->max_evictions > hive::kSlots || cfg->reserved != 0)
+        return HIVE_ERR_INVALID_ARG;
+    if (cfg->capacity_slots == 0) return HIVE_ERR_INVALID_ARG;
+    const uint64_t nb = (cfg->capacity_slots + hive::kSlots - 1) / hive::kSlots;
+    uint64_t nb_cap = std::max<uint64_t>(nb, (cfg->max_capacity_slots + hive::kSlots - 1) / hive::kSlots);
+    if (nb > 0x7FFFFFFFull || nb_cap > 0xFFFFFFFFull) return HIVE_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return HIVE_ERR_NO_DEVICE;
+    int dev = cfg->device;
+    if (dev < 0) HIVE_CUDA(cudaGetDevice(&dev));
+    if (dev >= ndev) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(dev);
+    if (!g.ok) return HIVE_ERR_CUDA;
+    hive_table* h = new (std::nothrow) hive_table();
+    if (!h) return HIVE_ERR_OOM;
+    h->device = dev;
+    h->policy = cfg->policy;
+    h->n0 = (uint32_t)nb;
+    Carve c = carve(nb_cap);
+    void* block = nullptr;
+    cudaError_t e = cudaMalloc(&block, c.total);
+    if (e != cudaSuccess) {
+        delete h;
+        return cuda_fail(e);
+    }
+    e = cudaMemset(block, 0, c.total);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cudaFree(block);
+        delete h;
+        return cuda_fail(e);
+    }
+    bind_arrays(h, block, nb_cap);
+    h->t.max_evictions = (uint32_t)cfg->max_evictions;
+    h->t.flags = 0;
+    set_geometry(h, 0, 0);
+    *out = h;
+    return HIVE_OK;
+}
+
+int hive_destroy(hive_table* h) {
+    if (!h) return HIVE_ERR_INVALID_ARG;
+    int rc = HIVE_OK;
+    if (h->block) {
+        DeviceGuard g(h->device);
+        cudaError_t e = cudaFree(h->block);
+        if (e != cudaSuccess) rc = cuda_fail(e);
+    }
+    delete h;
+    return rc;
+}
+
+int hive_clear(hive_table* h, void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = reset(h, s);
+    if (rc) return rc;
+    set_geometry(h, 0, 0);
+    h->t.flags = 0;
+    return HIVE_OK;
+}
+
+#define HIVE_DISPATCH(kern, grid, block, stream, ...)                                      \
+    do {                                                                                   \
+        if (h->policy == HIVE_POLICY_MURMURCITYHASH) kern<1><<<grid, block, 0, stream>>>(__VA_ARGS__); \
+        else kern<0><<<grid, block, 0, stream>>>(__VA_ARGS__);                             \
+    } while (0)
+
+int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uint64_t n, uint8_t* status,
+                void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n == 0) return HIVE_OK;
+    if (!keys || !values) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    HIVE_DISPATCH(k_insert, grid_for(n), kBlock, (cudaStream_t)stream, h->t, keys, values, n, status);
+    return launch_check();
+}
+
+int hive_find(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* values, uint8_t* found, void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n == 0) return HIVE_OK;
+    if (!keys) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    HIVE_DISPATCH(k_find, grid_for(n), kBlock, (cudaStream_t)stream, h->t, keys, n, values, found);
+    return launch_check();
+}
+
+int hive_erase(hive_table* h, const uint32_t* keys, uint64_t n, uint8_t* status, void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n == 0) return HIVE_OK;
+    if (!keys) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    h->t.flags |= hive::kFlagHoles;
+    HIVE_DISPATCH(k_erase, grid_for(n), kBlock, (cudaStream_t)stream, h->t, keys, n, status);
+    return launch_check();
+}
+
+int hive_apply_ops(hive_table* h, const uint8_t* types, const uint32_t* keys, const uint32_t* values, uint64_t n,
+                   uint8_t* status, uint32_t* out_values, uint32_t hints, void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n == 0) return HIVE_OK;
+    if (!types || !keys) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
+    HIVE_DISPATCH(k_apply, grid_for(n), kBlock, (cudaStream_t)stream, h->t, types, keys, values, n, status,
+                  out_values);
+    return launch_check();
+}
+
+int hive_apply_reference_ops(hive_table* h, const void* ops, uint64_t n, uint64_t* results, uint32_t hints,
+                             void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n == 0) return HIVE_OK;
+    if (!ops || ((uintptr_t)ops & 15)) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
+    HIVE_DISPATCH(k_apply_ref, grid_for(n), kBlock, (cudaStream_t)stream, h->t, (const ulonglong2*)ops, n,
+                  (unsigned long long*)results);
+    return launch_check();
+}
+
+int hive_size(hive_table* h, uint64_t* n_out, void* stream) {
+    if (!valid_table(h) || !n_out) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t nb = num_buckets(h);
+    HIVE_CUDA(cudaMemsetAsync(h->scratch, 0, 8, s));
+    k_count<<<grid_for(nb), kBlock, 0, s>>>(h->t, nb, h->scratch);
+    int rc = launch_check();
+    if (rc) return rc;
+    u64 v = 0;
+    HIVE_CUDA(cudaMemcpyAsync(&v, h->scratch, 8, cudaMemcpyDeviceToHost, s));
+    HIVE_CUDA(cudaStreamSynchronize(s));
+    *n_out = v;
+    return HIVE_OK;
+}
+
+int hive_dump(hive_table* h, uint64_t* kv, uint64_t cap, uint64_t* n_out, void* stream) {
+    if (!valid_table(h) || !n_out || (cap && !kv)) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t nb = num_buckets(h);
+    HIVE_CUDA(cudaMemsetAsync(h->scratch, 0, 8, s));
+    k_dump<<<grid_for(nb), kBlock, 0, s>>>(h->t, nb, (u64*)kv, cap, h->scratch);
+    int rc = launch_check();
+    if (rc) return rc;
+    u64 v = 0;
+    HIVE_CUDA(cudaMemcpyAsync(&v, h->scratch, 8, cudaMemcpyDeviceToHost, s));
+    HIVE_CUDA(cudaStreamSynchronize(s));
+    *n_out = v;
+    return HIVE_OK;
+}
+
+int hive_resize(hive_table* h, uint64_t target_slots, void* stream) {
+    if (!valid_table(h) || target_slots == 0) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    uint64_t target = (target_slots + hive::kSlots - 1) / hive::kSlots;
+    if (target > 0xFFFFFFFFull) return HIVE_ERR_CAPACITY;
+    if (target < h->n0) target = h->n0;  // never below the creation size (level 0)
+    if (target < num_buckets(h)) {
+        // A shrink is refused (table unchanged) unless the live entries fit the smaller table at
+        // load factor <= kMaxShrinkLoad, so the merge's re-inserts cannot run out of room.
+        uint64_t live = 0;
+        int rc = hive_size(h, &live, stream);
+        if (rc) return rc;
+        if ((double)live > kMaxShrinkLoad * (double)(target * hive::kSlots)) return HIVE_ERR_CAPACITY;
+    }
+    int rc = grow_capacity(h, target, s);
+    if (rc) return rc;
+    if (h->policy == HIVE_POLICY_MURMURCITYHASH) return resize_impl<1>(h, target, s);
+    return resize_impl<0>(h, target, s);
+}
+
+int hive_bucket_of(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* b0, uint32_t* b1, void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n == 0) return HIVE_OK;
+    if (!keys) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    HIVE_DISPATCH(k_bucket_of, grid_for(n), kBlock, (cudaStream_t)stream, h->t, keys, n, b0, b1);
+    return launch_check();
+}
+
+int hive_get_info(const hive_table* h, hive_info* out) {
+    if (!valid_table(h) || !out) return HIVE_ERR_INVALID_ARG;
+    std::memset(out, 0, sizeof(*out));
+    out->num_buckets = num_buckets(h);
+    out->capacity_slots = out->num_buckets * hive::kSlots;
+    out->max_buckets = h->nb_cap;
+    out->base_buckets = h->n0;
+    out->level = h->level;
+    out->split = h->t.split;
+    out->policy = h->policy;
+    out->max_evictions = (int32_t)h->t.max_evictions;
+    out->flags = h->t.flags;
+    out->device = h->device;
+    return HIVE_OK;
+}
+
+int hive_counters(hive_table* h, uint64_t* out, void* stream) {
+    if (!valid_table(h) || !out) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    HIVE_CUDA(cudaMemcpyAsync(out, h->t.counters, HIVE_NUM_COUNTERS * 8, cudaMemcpyDeviceToHost, s));
+    HIVE_CUDA(cudaStreamSynchronize(s));
+    return HIVE_OK;
+}
+
+int hive_check(hive_table* h, void* stream) {
+    uint64_t c[HIVE_NUM_COUNTERS];
+    int rc = hive_counters(h, c, stream);
+    if (rc) return rc;
+    if (c[HIVE_CTR_ERROR] & hive::kErrLockTimeout) return HIVE_ERR_LOCK_TIMEOUT;
+    if (c[HIVE_CTR_ERROR] & hive::kErrRetryOut) return HIVE_ERR_RETRY_LIMIT;
+    return HIVE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+/* hive_c.h -- C ABI of the B200 Hive hash table (32-bit keys, 32-bit values).
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status (HIVE_OK = 0), and
+ * never exits the process.  Key/value/status arrays are DEVICE pointers owned by the caller;
+ * work is enqueued on `stream` (a cudaStream_t passed as void*, NULL = legacy default stream)
+ * and is stream-ordered: outputs are valid once the stream has reached the call.  Calls that
+ * return a host value (hive_size, hive_dump's count, hive_counters, hive_check) synchronise
+ * `stream` first.  A table handle is not thread-safe; use one host thread per handle.
+ *
+ * Key 0 is reserved as the empty sentinel (reference include/utils.h:39-47): inserting it fails,
+ * looking it up or deleting it finds nothing.  Any other 32-bit key is valid.
+ *
+ * Each declaration cites the reference interface (SabbirPulok/HiveHashTable, path:line) that it
+ * replaces.  The reference's C++ entry points (hash_table_kernel_dispatch & co.) are rebuilt on
+ * top of this ABI in hivehashtable_b200/csrc/hive_compat.cpp.
+ */
+#ifndef HIVE_C_H
+#define HIVE_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden visibility; exactly the entry points below are exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---- status codes -------------------------------------------------------------------------- */
+#define HIVE_OK 0
+#define HIVE_ERR_INVALID_ARG 1   /* null handle/pointer, bad policy, size out of range        */
+#define HIVE_ERR_CUDA 2          /* a CUDA runtime call failed (see hive_last_cuda_error)     */
+#define HIVE_ERR_OOM 3           /* device allocation failed                                   */
+#define HIVE_ERR_LOCK_TIMEOUT 4  /* a bucket-lock wait expired inside a kernel (sticky)        */
+#define HIVE_ERR_RETRY_LIMIT 5   /* a CAS retry budget ran out inside a kernel (sticky)        */
+#define HIVE_ERR_CAPACITY 6      /* resize target beyond the reserved capacity                 */
+#define HIVE_ERR_NO_DEVICE 7     /* no CUDA device / the library was not built for it         */
+
+/* ---- hash policies (reference include/HashPolicies.cuh:10-17, :29-36) ------------------------ */
+#define HIVE_POLICY_DEFAULT2HASH 0   /* {hash1 (Wang), hash2 (Jenkins)} */
+#define HIVE_POLICY_MURMURCITYHASH 1 /* {murmurhash, cityhash}          */
+
+/* ---- per-op status bytes written by insert / erase / apply ----------------------------------- */
+#define HIVE_ST_FAIL 0      /* not placed (stash full, key 0) / not found                      */
+#define HIVE_ST_INSERTED 1  /* new key placed in a bucket; find/erase/increment: success       */
+#define HIVE_ST_UPDATED 2   /* existing key's value overwritten (upsert)                       */
+#define HIVE_ST_STASHED 3   /* new key placed in the overflow stash                            */
+#define HIVE_ST_ERROR 255   /* a bounded wait expired for this op                              */
+
+/* ---- op codes of hive_apply_ops (same numbering as reference OperationType, include/utils.h:10-16) */
+#define HIVE_OP_INSERT 0
+#define HIVE_OP_LOOKUP 1
+#define HIVE_OP_DELETE 2
+#define HIVE_OP_INCREMENT 3 /* the reference's ATOMIC_INC */
+#define HIVE_OP_NONE 4
+
+/* hints for hive_apply_ops / hive_apply_reference_ops */
+#define HIVE_HINT_NO_DELETES 1u /* caller guarantees the batch holds no DELETE op */
+
+/* ---- counters (hive_counters) ---------------------------------------------------------------- */
+#define HIVE_CTR_SLOW_PATH 0    /* inserts whose canonical bucket was full                     */
+#define HIVE_CTR_EVICTIONS 1    /* keys moved by cuckoo eviction                               */
+#define HIVE_CTR_STASH_PUSH 2   /* keys placed in the stash                                    */
+#define HIVE_CTR_FAILED 3       /* inserts that could not be placed                            */
+#define HIVE_CTR_LOCK_TIMEOUT 4 /* bucket-lock waits that expired                              */
+#define HIVE_CTR_RETRY_OUT 5    /* CAS retry budgets that ran out                              */
+#define HIVE_CTR_DUP_FIXED 6    /* duplicate copies removed after racing same-key inserts      */
+#define HIVE_CTR_ERROR 15       /* sticky error bits                                           */
+#define HIVE_NUM_COUNTERS 16
+
+typedef struct hive_table hive_table; /* opaque */
+
+typedef struct hive_config {
+    uint64_t capacity_slots;     /* slots at creation; buckets = ceil(capacity_slots / 8)        */
+    uint64_t max_capacity_slots; /* slots reserved for growth by hive_resize (0 = capacity)      */
+    int32_t policy;              /* HIVE_POLICY_*                                                */
+    int32_t max_evictions;       /* cuckoo victims tried per insert, 0..8 (reference default 8)  */
+    int32_t device;              /* CUDA device ordinal; -1 = the current device                 */
+    uint32_t reserved;           /* must be 0                                                    */
+} hive_config;
+
+typedef struct hive_info {
+    uint64_t num_buckets;     /* buckets in use (n_lo + split)                                */
+    uint64_t capacity_slots;  /* num_buckets * 8                                              */
+    uint64_t max_buckets;     /* buckets allocated                                            */
+    uint32_t base_buckets;    /* N0: buckets at level 0                                       */
+    uint32_t level;           /* linear-hashing level L (n_lo = N0 << L)                      */
+    uint32_t split;           /* buckets [0, split) already split at this level               */
+    int32_t policy;
+    int32_t max_evictions;
+    uint32_t flags;           /* bit 0: deletes or a resize ran since the last clear          */
+    int32_t device;
+    uint32_t reserved;
+} hive_info;
+
+/* Create a table with `capacity_slots` slots of zeroed HBM and room for max_capacity_slots.
+ * Replaces hiveHashTableCreate (include/hive_hash_table.cuh:92-113, src/hive_memory.cu:29-171),
+ * which sizes buckets from table_size / 8 the same way (src/hive_dispatch.cu:630-631). */
+int hive_create(const hive_config* cfg, hive_table** out);
+
+/* Free all device memory of the table.  Replaces hiveHashTableDestroy
+ * (include/hive_hash_table.cuh:115-128, src/hive_memory.cu:174-307). */
+int hive_destroy(hive_table* t);
+
+/* Empty the table (and its stash, locks, counters) and undo any resize.  Replaces
+ * hiveHashTableClear (include/hive_hash_table.cuh:141-143, src/hive_memory.cu:203-240). */
+int hive_clear(hive_table* t, void* stream);
+
+/* Bulk upsert of n (key, value) pairs; status[i] = HIVE_ST_*.  status may be NULL.
+ * Replaces hive_insert_kernel launched by run_hash_table_benchmark
+ * (include/hive_kernels.cuh:205-266, src/hive_dispatch.cu:134-148), with explicit values
+ * instead of the reference's value = key + 1 (include/hive_kernels.cuh:238). */
+int hive_insert(hive_table* t, const uint32_t* keys, const uint32_t* values, uint64_t n,
+                uint8_t* status, void* stream);
+
+/* Bulk lookup: values[i] = value of keys[i] (0 if absent), found[i] = 0/1.  Either output may be
+ * NULL.  Must not overlap on the GPU with a call that modifies the same table.
+ * Replaces hive_lookup_kernel (include/hive_kernels.cuh:76-117), which discards the value. */
+int hive_find(hive_table* t, const uint32_t* keys, uint64_t n, uint32_t* values, uint8_t* found,
+              void* stream);
+
+/* Bulk delete of every copy of each key; status[i] = 1 removed, 0 absent.  status may be NULL.
+ * Replaces the DELETE case of hive_mixed_kernel (include/hive_kernels.cuh:177-181,
+ * include/hive_hash_delete.cuh:168-194). */
+int hive_erase(hive_table* t, const uint32_t* keys, uint64_t n, uint8_t* status, void* stream);
+
+/* Mixed batch, ops unordered within the call: types[i] = HIVE_OP_*, values used by INSERT.
+ * status[i] = HIVE_ST_* (lookup/delete/increment: 1 success, 0 miss); out_values[i] = value
+ * found (LOOKUP) or value after the increment (INCREMENT), else 0.  out_values/status may be
+ * NULL.  hints: HIVE_HINT_*.
+ * Replaces hive_mixed_kernel (include/hive_kernels.cuh:119-192) with structure-of-arrays input. */
+int hive_apply_ops(hive_table* t, const uint8_t* types, const uint32_t* keys, const uint32_t* values,
+                   uint64_t n, uint8_t* status, uint32_t* out_values, uint32_t hints, void* stream);
+
+/* Mixed batch in the reference's own record layout: ops points to n 16-byte records
+ * {int32 type (OperationType); 4 bytes padding; uint64 key} (include/utils.h:18-21);
+ * value = (uint32)key + 1 (include/hive_kernels.cuh:156); results[i] = 1 on success else 0,
+ * as uint64 (include/hive_kernels.cuh:187-190).  results may be NULL.
+ * Replaces hive_mixed_kernel / hive_insert_kernel / hive_lookup_kernel as launched by
+ * run_hash_table_benchmark (src/hive_dispatch.cu:119-162). */
+int hive_apply_reference_ops(hive_table* t, const void* ops, uint64_t n, uint64_t* results,
+                             uint32_t hints, void* stream);
+
+/* Number of live entries (buckets + stash).  Synchronises `stream`.  Replaces
+ * count_occupancy_kernel (include/hive_kernels.cuh:303-325), which counts freeMask bits. */
+int hive_size(hive_table* t, uint64_t* n_out, void* stream);
+
+/* Copy up to `cap` packed entries ((value << 32) | key, arbitrary order) to the device array kv;
+ * *n_out = total number of entries (may exceed cap).  Synchronises `stream`.  No reference
+ * counterpart: the reference has no way to read its table back (its compact_stash_kernel,
+ * include/hive_stash_table.cuh:33-64, does this for the stash only). */
+int hive_dump(hive_table* t, uint64_t* kv, uint64_t cap, uint64_t* n_out, void* stream);
+
+/* Grow or shrink to ceil(target_slots / 8) buckets by linear-hashing split/merge, stream-ordered
+ * between other calls (synchronises `stream`).  Growth beyond the reserved capacity reallocates.
+ * A shrink stops at the creation size and is refused with HIVE_ERR_CAPACITY (table unchanged)
+ * when the live entries would exceed load factor 0.9 of the target.
+ * Replaces hive_hash_grow / hive_hash_shrink (include/hive_hash_resize.cuh:138-215, :340-420). */
+int hive_resize(hive_table* t, uint64_t target_slots, void* stream);
+
+/* Diagnostic: the two candidate buckets of each key (device arrays) under the table's current
+ * geometry.  Replaces HashPolicy::get_bucket(0|1, key, num_buckets)
+ * (include/HashPolicies.cuh:13-16, :32-35). */
+int hive_bucket_of(hive_table* t, const uint32_t* keys, uint64_t n, uint32_t* b0, uint32_t* b1, void* stream);
+
+/* Table geometry.  Host only, no device work. */
+int hive_get_info(const hive_table* t, hive_info* out);
+
+/* Copy the HIVE_NUM_COUNTERS device counters to host memory `out`.  Synchronises `stream`.
+ * Replaces the per-stage InsertBreakdown timing of -DBREAKDOWN_INSERT
+ * (include/hive_hash_table_struct.cuh:274-294, src/hive_dispatch.cu:268-312) with event counts. */
+int hive_counters(hive_table* t, uint64_t* out, void* stream);
+
+/* Synchronise `stream` and report a sticky in-kernel error: HIVE_ERR_LOCK_TIMEOUT or
+ * HIVE_ERR_RETRY_LIMIT if any op hit its bound since the last clear, else HIVE_OK.
+ * The reference has no counterpart (its lock spins are unbounded,
+ * include/hive_hash_table_struct.cuh:101-117). */
+int hive_check(hive_table* t, void* stream);
+
+/* Message for a status code; never NULL. */
+const char* hive_strerror(int status);
+
+/* The cudaError_t (as int) of the last failing CUDA call on this thread, 0 if none. */
+int hive_last_cuda_error(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIVE_C_H */

@@ -1,0 +1,90 @@
+"""TEST INFRASTRUCTURE: build recipe for the oracle and for the reference-side pins.
+
+  oracle/lib/libhive_oracle.so        the CPU restatement (hive_oracle.cpp), g++
+  oracle/_ref/hash_kat_inc            reference include/hash.hpp host hashes   (needs the reference tree)
+  oracle/_ref/hash_kat_uhf            reference UniformHashFunction hash_function.cu (plain-C hash2)
+  oracle/_ref/libhive_ref_hashdev.so  reference device hash policies, sm_100a
+
+The reference is compiled directly from its sources where they lie (REFERENCE_ROOT, default
+/root/reference); nothing is copied into this repository and the reference's own build system is
+not used.  Outputs under oracle/_ref/ are git-ignored but travel with the source tree, so the GPU
+tests can use the prebuilt reference library where the reference tree is absent.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "lib"
+REF_OUT = HERE / "_ref"
+REFERENCE_ROOT = Path(os.environ.get("HIVE_REFERENCE_ROOT", "/root/reference"))
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for c in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if c and Path(c).exists():
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _run(cmd):
+    p = subprocess.run([str(c) for c in cmd], capture_output=True, text=True)
+    if p.returncode:
+        sys.stderr.write(p.stdout + p.stderr)
+        raise RuntimeError("oracle build step failed: " + " ".join(map(str, cmd)))
+
+
+def _stale(out: Path, deps) -> bool:
+    return not out.exists() or any(Path(d).stat().st_mtime > out.stat().st_mtime for d in deps)
+
+
+def build_oracle(force: bool = False) -> Path:
+    out = LIB / "libhive_oracle.so"
+    src = HERE / "hive_oracle.cpp"
+    if force or _stale(out, [src]):
+        LIB.mkdir(exist_ok=True)
+        _run(["g++", "-O3", "-std=c++17", "-shared", "-fPIC", "-pthread", src, "-o", out])
+    return out
+
+
+def reference_available() -> bool:
+    return (REFERENCE_ROOT / "include" / "hash.hpp").exists()
+
+
+def build_reference_pins(force: bool = False) -> list[Path]:
+    """Compile the reference's hash code into oracle/_ref (only where the reference tree exists)."""
+    if not reference_available():
+        return []
+    REF_OUT.mkdir(exist_ok=True)
+    inc = REFERENCE_ROOT / "include"
+    uhf = REFERENCE_ROOT / "UniformHashFunction"
+    outs = []
+    o = REF_OUT / "hash_kat_inc"
+    if force or _stale(o, [HERE / "ref" / "hash_kat_inc.cpp", inc / "hash.hpp"]):
+        _run([_nvcc(), "-std=c++17", "-O2", "-x", "cu", f"-I{inc}", HERE / "ref" / "hash_kat_inc.cpp", "-o", o])
+    outs.append(o)
+    o = REF_OUT / "hash_kat_uhf"
+    if force or _stale(o, [HERE / "ref" / "hash_kat_uhf.cpp", uhf / "src" / "hash_function.cu"]):
+        _run([_nvcc(), "-std=c++17", "-O2", f"-I{uhf / 'include'}", "-x", "cu", HERE / "ref" / "hash_kat_uhf.cpp",
+              "-x", "cu", uhf / "src" / "hash_function.cu", "-o", o])
+    outs.append(o)
+    o = REF_OUT / "libhive_ref_hashdev.so"
+    if force or _stale(o, [HERE / "ref" / "hash_dev_kat.cu", inc / "hash.hpp", inc / "HashPolicies.cuh"]):
+        _run([_nvcc(), *ARCH, "-std=c++17", "-O3", "-shared", "-Xcompiler", "-fPIC", f"-I{inc}",
+              HERE / "ref" / "hash_dev_kat.cu", "-o", o])
+    outs.append(o)
+    return outs
+
+
+def build_all(force: bool = False) -> list[Path]:
+    return [build_oracle(force), *build_reference_pins(force)]
+
+
+if __name__ == "__main__":
+    for p in build_all(force="--force" in sys.argv):
+        print(p)

@@ -1,0 +1,334 @@
+"""CUDA path vs the oracle, bit-exact, through the C ABI (libhive_b200.so).
+
+Small and medium cases are compared op by op with the std::unordered_map replay and by the full
+key->value set (hive_dump); the full-size case is checked through size-independent properties.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from hivehashtable_b200 import (OP_DELETE, OP_INCREMENT, OP_INSERT, OP_LOOKUP, OP_NONE, ST_ERROR, ST_FAIL, HiveError,
+                                ST_INSERTED, ST_STASHED, ST_UPDATED, HiveHashTable, u32)
+from hivehashtable_b200 import workload
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+POLICIES = ["Default2Hash", "MurmurCityHash"]
+
+
+def _np(t):
+    return t.cpu().numpy()
+
+
+def _assert_same_set(table: HiveHashTable, m: oracle.ReplayMap):
+    gk, gv = table.dump()
+    ok, ov = m.dump()
+    assert gk.size == ok.size, (gk.size, ok.size)
+    np.testing.assert_array_equal(gk, ok)
+    np.testing.assert_array_equal(gv, ov)
+    assert table.size() == len(m)
+
+
+def _insert_and_check(table, m, keys, vals):
+    st = _np(table.insert(keys, vals))
+    assert not (st == ST_ERROR).any()
+    exp = m.insert(keys, vals, apply_mask=(st != ST_FAIL).astype(np.uint8))
+    ok = st != ST_FAIL
+    # inserted/stashed <-> new key, updated <-> existing key
+    np.testing.assert_array_equal(np.where(st[ok] == ST_UPDATED, 2, 1), exp[ok])
+    return st
+
+
+def _find_and_check(table, m, keys):
+    v, f = table.find(keys)
+    ev, ef = m.find(keys)
+    np.testing.assert_array_equal(_np(f), ef)
+    np.testing.assert_array_equal(u32(v), ev)
+    return _np(f)
+
+
+@pytest.mark.parametrize("policy", POLICIES)
+def test_golden_bulk_small(cuda, policy):
+    g = np.load(GOLD / "bulk_small.npz")
+    with HiveHashTable(int(g["capacity"]), policy) as t:
+        st = _np(t.insert(g["keys"], g["values"]))
+        np.testing.assert_array_equal(st != ST_FAIL, g["insert_status"] == 1)
+        assert set(np.unique(st).tolist()) <= {ST_INSERTED, ST_STASHED}
+        v, f = t.find(g["lookup_keys"])
+        np.testing.assert_array_equal(_np(f), g["found"])
+        np.testing.assert_array_equal(u32(v), g["found_values"])
+        k, vals = t.dump()
+        order = np.argsort(g["keys"])
+        np.testing.assert_array_equal(k, g["keys"][order])
+        np.testing.assert_array_equal(vals, g["values"][order])
+        t.check()
+
+
+def test_plain_bulk_small_config(cuda):
+    """2^20 unique keys (seed 42) into a table sized for LF 0.8, Default2Hash; 2^20 lookups with
+    half present, shuffled; every result bit-exact against the replay."""
+    n = 1 << 20
+    cap = -(-n * 10 // 8)
+    keys, absent, st = oracle.gen_keys(42, n, n // 2)
+    vals = oracle.values_for(keys)
+    look, _ = oracle.lookup_set(keys, absent, n // 2, n // 2, st)
+    m = oracle.ReplayMap()
+    with HiveHashTable(cap, "Default2Hash") as t:
+        ins = _insert_and_check(t, m, keys, vals)
+        assert (ins != ST_FAIL).all()
+        f = _find_and_check(t, m, look)
+        assert f.sum() == n // 2
+        _assert_same_set(t, m)
+        t.check()
+
+
+@pytest.mark.parametrize("policy", POLICIES)
+@pytest.mark.parametrize("cap_log", [16, 20])
+@pytest.mark.parametrize("lf", [0.65, 0.80, 0.90, 0.95, 1.0])
+def test_bulk_sweep(cuda, policy, cap_log, lf):
+    cap = 1 << cap_log
+    n = int(lf * cap)
+    keys, absent, st = oracle.gen_keys(7, n, n)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(cap, policy) as t:
+        ins = _insert_and_check(t, m, keys, vals)
+        failed = int((ins == ST_FAIL).sum())
+        if lf <= 0.95:
+            assert failed == 0, failed
+        c = t.counters()
+        assert c["failed"] == failed and c["error_bits"] == 0
+        for p in (0.0, 0.25, 0.5, 0.75, 1.0):
+            npres = int(round(p * min(n, 1 << 14)))
+            nabs = min(n, 1 << 14) - npres
+            look, st = oracle.lookup_set(keys, absent, npres, nabs, st)
+            _find_and_check(t, m, look)
+        _assert_same_set(t, m)
+
+
+def test_reference_record_path(cuda):
+    """16-byte Operation records, value = key + 1, uint64 0/1 results (the reference's kernel
+    contract, include/hive_kernels.cuh:119-266)."""
+    n = 50_000
+    keys, absent, _ = oracle.gen_keys(11, n, n // 4)
+    ops = np.zeros((n, 2), dtype=np.int64)
+    ops[:, 0] = 0
+    ops[:, 1] = keys.astype(np.int64)
+    with HiveHashTable(1 << 17) as t:
+        r = _np(t.apply_reference_ops(torch.from_numpy(ops), hints=1))
+        assert (r == 1).all()
+        look = np.concatenate([keys[: n // 2], absent])
+        lops = np.stack([np.full(look.size, 1, np.int64), look.astype(np.int64)], axis=1)
+        r = _np(t.apply_reference_ops(torch.from_numpy(lops)))
+        np.testing.assert_array_equal(r, np.r_[np.ones(n // 2), np.zeros(absent.size)].astype(np.int64))
+        v, f = t.find(keys[:100])
+        np.testing.assert_array_equal(u32(v), keys[:100] + np.uint32(1))
+        # delete / ATOMIC_INC (3) / NONE (4) records
+        dops = np.stack([np.array([2, 2, 3, 3, 4], np.int64),
+                         np.array([keys[0], absent[0], keys[1], absent[1], keys[2]], np.int64)], axis=1)
+        r = _np(t.apply_reference_ops(torch.from_numpy(dops)))
+        assert r.tolist() == [1, 0, 1, 0, 0]
+        v, f = t.find(keys[:3])
+        assert _np(f).tolist() == [0, 1, 1] and u32(v)[1] == keys[1] + 2
+
+
+@pytest.mark.parametrize("policy", POLICIES)
+def test_erase_then_reinsert(cuda, policy):
+    n = 200_000
+    cap = int(n / 0.9)
+    keys, absent, st = oracle.gen_keys(13, n, n // 2)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(cap, policy) as t:
+        _insert_and_check(t, m, keys, vals)
+        gone = keys[::2]
+        est = _np(t.erase(np.concatenate([gone, absent[:1000], [0]])))
+        exp = m.erase(np.concatenate([gone, absent[:1000], [0]]))
+        np.testing.assert_array_equal(est, exp)
+        _assert_same_set(t, m)
+        # holes mode: upserts of survivors, re-inserts of erased keys, new keys
+        mix = np.concatenate([keys[1:20000:2], gone[:20000], absent[:20000]])
+        _insert_and_check(t, m, mix, oracle.values_for(mix) ^ np.uint32(0x5A5A5A5A))
+        look, _ = oracle.lookup_set(keys, absent, 50_000, 50_000, st)
+        _find_and_check(t, m, look)
+        _assert_same_set(t, m)
+        assert t.info()["flags"] & 1
+
+
+@pytest.mark.parametrize("policy", POLICIES)
+def test_mixed_batches(cuda, policy):
+    """Batches of 50 % insert (new keys), 40 % lookup (80 % present), 10 % delete (present keys,
+    disjoint from the lookups); at most one op per key per batch, so every op's result is fixed."""
+    rng_state = 11
+    pre, pool, rng_state = oracle.gen_keys(rng_state, 60_000, 400_000)
+    m = oracle.ReplayMap()
+    live = list(pre)
+    with HiveHashTable(1 << 17, policy) as t:
+        _insert_and_check(t, m, pre, oracle.values_for(pre))
+        pool_i = 0
+        rs = np.random.RandomState(5)
+        for b in range(12):
+            size = int(2 ** rs.uniform(10, 15))
+            ni, nl, nd = size // 2, size * 4 // 10, size - size // 2 - size * 4 // 10
+            new = pool[pool_i: pool_i + ni]
+            pool_i += ni
+            livea = np.array(live, dtype=np.uint32)
+            sel = rs.choice(livea.size, size=nl + nd, replace=False)
+            lk_present = livea[sel[: int(nl * 0.8)]]
+            lk_absent = pool[pool_i: pool_i + (nl - lk_present.size)]
+            pool_i += lk_absent.size
+            dels = livea[sel[nl: nl + nd]]
+            keys = np.concatenate([new, lk_present, lk_absent, dels]).astype(np.uint32)
+            types = np.concatenate([np.full(ni, OP_INSERT), np.full(nl, OP_LOOKUP), np.full(nd, OP_DELETE)]).astype(np.uint8)
+            vals = oracle.values_for(keys)
+            perm = rs.permutation(keys.size)
+            keys, types, vals = keys[perm], types[perm], vals[perm]
+            st, ov = t.apply(types, keys, vals)
+            st, ov = _np(st), u32(ov)
+            assert not (st == ST_ERROR).any()
+            ok_ins = (types != OP_INSERT) | (st != ST_FAIL)
+            est, eov = m.apply(types, keys, vals, apply_mask=ok_ins.astype(np.uint8))
+            gst = np.where((types == OP_INSERT) & (st == ST_STASHED), 1, st)
+            np.testing.assert_array_equal(gst, est)
+            np.testing.assert_array_equal(ov, eov)
+            live = sorted((set(live) | set(new.tolist())) - set(dels.tolist()))
+        _assert_same_set(t, m)
+        t.check()
+
+
+def test_duplicate_keys_in_one_batch(cuda):
+    keys = np.repeat(np.arange(1, 5001, dtype=np.uint32) * np.uint32(2654435761), 3)
+    vals = np.arange(keys.size, dtype=np.uint32)
+    perm = np.random.RandomState(1).permutation(keys.size)
+    keys, vals = keys[perm], vals[perm]
+    with HiveHashTable(1 << 14) as t:
+        st = _np(t.insert(keys, vals))
+        assert (st != ST_FAIL).all()
+        for k in np.unique(keys)[:200]:
+            s = st[keys == k]
+            assert ((s == ST_INSERTED) | (s == ST_STASHED)).sum() == 1 and (s == ST_UPDATED).sum() == 2
+        gk, gv = t.dump()
+        assert gk.size == np.unique(keys).size and np.unique(gk).size == gk.size
+        for k, v in zip(gk[:500], gv[:500]):
+            assert v in vals[keys == k]
+
+
+def test_key_zero_and_empty_inputs(cuda):
+    with HiveHashTable(1024) as t:
+        e = np.zeros(0, np.uint32)
+        assert t.insert(e, e).numel() == 0
+        assert t.find(e)[0].numel() == 0
+        assert _np(t.insert([0, 5], [9, 9])).tolist() == [ST_FAIL, ST_INSERTED]
+        v, f = t.find([0, 5])
+        assert _np(f).tolist() == [0, 1] and u32(v).tolist() == [0, 9]
+        assert _np(t.erase([0])).tolist() == [0]
+        st, ov = t.apply([OP_NONE, OP_LOOKUP, OP_INCREMENT, OP_INCREMENT], [5, 0, 5, 6], [0, 0, 0, 0])
+        assert _np(st).tolist() == [0, 0, 1, 0] and u32(ov).tolist() == [0, 0, 10, 0]
+        assert t.size() == 1
+        t.clear()
+        assert t.size() == 0 and _np(t.find([5])[1]).tolist() == [0]
+
+
+@pytest.mark.parametrize("max_ev", [0, 8])
+def test_forced_collisions_stash_and_overflow(cuda, max_ev):
+    """64 slots (8 buckets) and 300 keys: the stash fills and inserts fail; the successful set and
+    every lookup still match the replay exactly."""
+    keys, absent, _ = oracle.gen_keys(3, 300, 100)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(64, max_evictions=max_ev) as t:
+        st = _insert_and_check(t, m, keys, vals)
+        assert (st == ST_FAIL).sum() > 0 and (st == ST_STASHED).sum() > 0
+        c = t.counters()
+        assert c["stash_push"] == (st == ST_STASHED).sum() and c["failed"] == (st == ST_FAIL).sum()
+        _find_and_check(t, m, np.concatenate([keys, absent]))
+        _assert_same_set(t, m)
+        # erase stashed keys and re-insert: stash slots are reused
+        _np(t.erase(keys[:150]))
+        m.erase(keys[:150])
+        _assert_same_set(t, m)
+        st2 = _insert_and_check(t, m, keys[:150], vals[:150] + np.uint32(1))
+        assert (st2 != ST_FAIL).sum() > 0
+        _find_and_check(t, m, np.concatenate([keys, absent]))
+        _assert_same_set(t, m)
+
+
+@pytest.mark.parametrize("policy", POLICIES)
+def test_resize_grow_and_shrink(cuda, policy):
+    keys, absent, st = oracle.gen_keys(13, 120_000, 20_000)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(1 << 14, policy) as t:
+        done = 0
+        for chunk in range(12):
+            part = keys[done: done + 10_000]
+            done += part.size
+            info = t.info()
+            if (len(m) + part.size) / info["capacity_slots"] > 0.85:
+                t.resize(info["capacity_slots"] * 2)
+                _assert_same_set(t, m)
+            _insert_and_check(t, m, part, vals[done - part.size: done])
+            _assert_same_set(t, m)
+        inf = t.info()
+        assert inf["capacity_slots"] > (1 << 14) and inf["num_buckets"] == inf["capacity_slots"] // 8
+        # odd intermediate size (split pointer mid-level), then shrink
+        t.resize(inf["capacity_slots"] + 8 * 1000)
+        _assert_same_set(t, m)
+        look, _ = oracle.lookup_set(keys, absent, 20_000, 20_000, st)
+        _find_and_check(t, m, look)
+        gone = keys[: 100_000]
+        np.testing.assert_array_equal(_np(t.erase(gone)), m.erase(gone))
+        t.resize(1 << 15)
+        assert t.info()["capacity_slots"] == 1 << 15
+        _assert_same_set(t, m)
+        _find_and_check(t, m, look)
+        # 20,000 live keys do not fit 2^14 slots at LF <= 0.9: refused, table unchanged
+        with pytest.raises(HiveError) as e:
+            t.resize(1 << 10)
+        assert e.value.code == 6 and t.info()["capacity_slots"] == 1 << 15
+        _assert_same_set(t, m)
+        more = keys[100_000: 110_000]
+        np.testing.assert_array_equal(_np(t.erase(more)), m.erase(more))
+        t.resize(1 << 10)  # clamped to the creation size
+        assert t.info()["capacity_slots"] == 1 << 14
+        _assert_same_set(t, m)
+        _find_and_check(t, m, look)
+        t.check()
+
+
+def test_bucket_choice_matches_oracle(cuda):
+    keys = np.random.RandomState(0).randint(0, 2**32, size=100_000, dtype=np.uint64).astype(np.uint32)
+    for policy, pid in (("Default2Hash", 0), ("MurmurCityHash", 1)):
+        for cap in (8, 1_310_720, 1 << 26):
+            with HiveHashTable(cap, policy) as t:
+                b0, b1 = t.bucket_of(keys)
+                e0, e1 = oracle.buckets(pid, keys, t.info()["num_buckets"])
+                np.testing.assert_array_equal(u32(b0), e0)
+                np.testing.assert_array_equal(u32(b1), e1)
+
+
+def test_full_size_properties(cuda):
+    """Headline size: 2^26 slots at LF 0.9 (60,397,977 keys, seed 7).  Size-independent checks:
+    every insert succeeds, size equals n, every inserted key is found with its own value, absent
+    keys are missed, and the dump's key and value checksums equal the inputs'."""
+    cap = 1 << 26
+    n = int(0.9 * cap)
+    keys, absent, _ = workload.gen_keys(7, n, 1 << 20)
+    vals = workload.values_for(keys)
+    with HiveHashTable(cap) as t:
+        st = _np(t.insert(keys, vals))
+        assert (st != ST_FAIL).all() and not (st == ST_UPDATED).any()
+        assert t.size() == n
+        v, f = t.find(keys)
+        assert bool((f == 1).all())
+        np.testing.assert_array_equal(u32(v), vals)
+        _, fa = t.find(absent)
+        assert int(fa.sum()) == 0
+        gk, gv = t.dump()
+        assert gk.size == n and np.unique(gk).size == n
+        assert int(gk.astype(np.uint64).sum()) == int(keys.astype(np.uint64).sum())
+        assert int(gv.astype(np.uint64).sum()) == int(vals.astype(np.uint64).sum())
+        t.check()
