@@ -230,6 +230,7 @@ def main():
     placed = int((st != 0).sum())
     assert placed == n and int(fnd.sum()) == n_present, (placed, n, int(fnd.sum()), n_present)
     table.check()
+    step_counters = table.counters()
 
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -327,7 +328,8 @@ def main():
                 "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seeded uint32 keys/values)",
                 "config": workload_config(args, world), "roofline": roof, "roofline_all": rl,
                 "insert_mops": rl["k_insert"]["mops"], "lookup_mops": rl["k_find"]["mops"],
-                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": 3 * args.steps,
+                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": 4 * args.steps,
+                "insert_counters": step_counters,
                 "clocks": sampler.summary()}
         print(json.dumps(line), flush=True)
     table.close()

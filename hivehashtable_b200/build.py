@@ -75,7 +75,7 @@ def build_compat(force: bool = False) -> Path:
     core = build_core(force=False)
     if force or _stale(out, [src, core, *hdrs]):
         LIB.mkdir(exist_ok=True)
-        _run([_nvcc(), "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", f"-I{INCLUDE}",
+        _run([_nvcc(), "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", f"-I{INCLUDE}", f"-I{CSRC / 'compat_types'}",
               str(src), "-o", str(out), f"-L{LIB}", "-lhive_b200", "-Xlinker", "-rpath=$ORIGIN", "-lcudart"])
     return out
 

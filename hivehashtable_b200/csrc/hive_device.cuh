@@ -35,6 +35,7 @@ enum : uint8_t {
     kStInserted = 1,  // insert placed a new key in a bucket; find/erase/increment: success
     kStUpdated = 2,   // insert overwrote the value of an existing key (upsert)
     kStStashed = 3,   // insert placed a new key in the overflow stash
+    kStDefer = 0xFE,  // internal: the op needs the locked path and was queued for the second pass
     kStError = 0xFF,  // a bounded wait expired (lock timeout or retry budget spent)
 };
 
@@ -348,21 +349,25 @@ __device__ __forceinline__ bool resolve_duplicate(const Table& t, u64* p, uint32
 // ---------------------------------------------------------------------------------------------
 // Insert = upsert (S2).  Four stages as in include/hive_hash_insert.cuh:898-1042:
 //   A  try-replace in the candidate buckets and the canonical stash,
-//   B  claim a free slot of the canonical bucket H0 with a 64-bit CAS,
+//   B  claim a free slot with a 64-bit CAS: in the canonical bucket H0, and when H0 is full in
+//      the key's other bucket H1 (the reference claims in H0 only and goes straight to C),
 //   C  bounded depth-1 cuckoo eviction from H0 under H0's lock,
 //   D  the canonical bucket's overflow stash.
 //
 // Invariants that keep every key in exactly one place and visible at all times:
-//   * a new key is only ever placed in its canonical bucket H0 (or H0's stash);
+//   * a new key is placed in H0, in H1 only when H0 is full, else in H0's stash;
 //   * a victim is moved only from its own H0 to its H1, and is written to H1 before its H0 slot
 //     is overwritten, so a reader scanning H0 then H1 always sees it;
 //   * an evictor holds H0's lock, so one victim has one mover;
 //   * every slot change is a CAS from an observed value, so a concurrent update or delete of
 //     the victim is detected and either propagated to the copy or undone.
 // Without kFlagHoles (no delete or resize since the last clear) slots only ever go from free to
-// occupied, so a key can live in H1 or in the stash only if H0 is full: stage B may then claim in
-// H0 without reading H1 first, and two inserts of one key always race for the same lowest free
-// slot (so they cannot both succeed).
+// occupied and every claimer (new keys and moved victims alike) takes the lowest free slot, so:
+//   * a key lives in H1 only if H0 is full, and in the stash only if H0 and H1 are both full;
+//   * stage B needs no lock: two inserts of one key race for the same lowest free slot of the
+//     same bucket, one CAS wins and the other re-reads the bucket and finds the key.
+// Ops that reach stages C/D (both buckets full) can be deferred by the first pass to a queue that
+// a second, compact pass finishes, so a warp of one-op threads does not wait on its slowest lane.
 // ---------------------------------------------------------------------------------------------
 
 enum { kEvPlaced = 1, kEvRetry = 2, kEvNone = 0 };
@@ -454,6 +459,15 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
             }
             continue;
         }
+        e = b1 != b0 ? empty_mask(B1) : 0u;
+        if (e) {
+            int j = __ffs(e) - 1;
+            if (cas64(B1p + j, 0ull, kv) == 0ull) {
+                if (holes && resolve_duplicate(t, B1p, k, j, kv)) return kStUpdated;
+                return kStInserted;
+            }
+            continue;
+        }
         int ev = try_evict<P>(t, B0p, B0, b0, kv);
         if (ev == kEvPlaced) return kStInserted;
         if (ev == kEvRetry) continue;
@@ -482,74 +496,102 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
     return kStError;
 }
 
-template <int P>
-__device__ __noinline__ uint8_t insert_slow(const Table& t, uint32_t k, u64 kv, uint32_t b0) {
-    const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
-    const bool holes = t.flags & kFlagHoles;
+// Without holes: update k in bucket p or claim p's lowest free slot.  Returns kStUpdated /
+// kStInserted, or 0 when p is full (or its retry budget ran out: the locked path finishes).
+__device__ __forceinline__ uint8_t claim_or_update(u64* p, uint32_t k, u64 kv) {
+    for (int r = 0; r < kRetryLimit; ++r) {
+        Bucket B;
+        load_bucket(p, B);
+        uint32_t m = match_mask(B, k);
+        if (m) {
+            int j = __ffs(m) - 1;
+            u64 old = slot_at(B, j);
+            if (cas64(p + j, old, kv) == old) return kStUpdated;
+            continue;
+        }
+        uint32_t e = empty_mask(B);
+        if (!e) return 0;
+        if (cas64(p + (__ffs(e) - 1), 0ull, kv) == 0ull) return kStInserted;
+    }
+    return 0;
+}
+
+// Which insert protocol a kernel compiles: chosen from the table's flags at run time, or fixed
+// by the host (which knows the flags) so the kernel carries only the code it needs.
+enum Mode { kModeRuntime = 0, kModeMono = 1, kModeHoles = 2 };
+
+// Lock-free stages A and B.  Returns the op's final status, or 0 when H0 and H1 are both full
+// and the locked path (stages C/D) is needed.
+template <int P, int kMode = kModeRuntime>
+__device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
     u64* B0p = t.slots + (size_t)b0 * kSlots;
     u64* B1p = t.slots + (size_t)b1 * kSlots;
+    const bool holes = kMode == kModeHoles || (kMode == kModeRuntime && (t.flags & kFlagHoles));
+    if (!holes) {
+        uint8_t st = claim_or_update(B0p, k, kv);
+        if (st || b1 == b0) return st;
+        return claim_or_update(B1p, k, kv);
+    }
+    // With holes a key may sit in H1 or the stash while H0 has room: scan all three first.
     u64* Sp = t.stash + (size_t)b0 * kSlots;
-    count(t, kCtrSlowPath);
-    // Lock-free stage A over H1 and the stash; with holes also stage B in H0.
     for (int r = 0; r < kRetryLimit; ++r) {
-        int u = update_in(B0p, k, kv);
-        if (u == 1) return kStUpdated;
-        if (u < 0) continue;
-        if (b1 != b0) {
-            u = update_in(B1p, k, kv);
-            if (u == 1) return kStUpdated;
-            if (u < 0) continue;
+        Bucket B0, B1;
+        load_bucket(B0p, B0);
+        load_bucket(B1p, B1);
+        uint32_t m = match_mask(B0, k);
+        if (m) {
+            int j = __ffs(m) - 1;
+            u64 old = slot_at(B0, j);
+            if (cas64(B0p + j, old, kv) == old) return kStUpdated;
+            continue;
+        }
+        m = match_mask(B1, k);
+        if (m) {
+            int j = __ffs(m) - 1;
+            u64 old = slot_at(B1, j);
+            if (cas64(B1p + j, old, kv) == old) return kStUpdated;
+            continue;
         }
         if (stash_flag(t, b0)) {
-            u = update_in(Sp, k, kv);
+            int u = update_in(Sp, k, kv);
             if (u == 1) return kStUpdated;
             if (u < 0) continue;
         }
-        if (holes) {
-            Bucket B0;
-            load_bucket(B0p, B0);
-            uint32_t e = empty_mask(B0);
-            if (match_mask(B0, k)) continue;
-            if (e) {
-                int j = __ffs(e) - 1;
-                if (cas64(B0p + j, 0ull, kv) == 0ull) {
-                    if (resolve_duplicate(t, B0p, k, j, kv)) return kStUpdated;
-                    return kStInserted;
-                }
-                continue;
-            }
+        uint32_t e = empty_mask(B0);
+        u64* Cp = B0p;
+        if (!e && b1 != b0) {
+            e = empty_mask(B1);
+            Cp = B1p;
         }
-        break;
+        if (!e) return 0;
+        int j = __ffs(e) - 1;
+        if (cas64(Cp + j, 0ull, kv) == 0ull) return resolve_duplicate(t, Cp, k, j, kv) ? kStUpdated : kStInserted;
     }
+    return 0;
+}
+
+// Stages C/D: H0's lock, a rescan, eviction, the stash.
+template <int P>
+__device__ __noinline__ uint8_t insert_locked_path(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
+    count(t, kCtrSlowPath);
     if (!lock_bucket(t, b0)) return kStError;
     uint8_t st = insert_locked<P>(t, k, kv, b0, b1);
     unlock_bucket(t, b0);
     return st;
 }
 
-template <int P>
+// One upsert.  With kDefer, an op that needs the locked path returns kStDefer untouched (and the
+// locked path is not compiled into the caller).
+template <int P, bool kDefer = false, int kMode = kModeRuntime>
 __device__ __forceinline__ uint8_t insert_one(const Table& t, uint32_t k, uint32_t v) {
     if (k == 0) return kStFail;
     const u64 kv = pack(k, v);
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
-    if (!(t.flags & kFlagHoles)) {
-        u64* B0p = t.slots + (size_t)b0 * kSlots;
-        for (int r = 0; r < kRetryLimit; ++r) {
-            Bucket B;
-            load_bucket(B0p, B);
-            uint32_t m = match_mask(B, k);
-            if (m) {
-                int j = __ffs(m) - 1;
-                u64 old = slot_at(B, j);
-                if (cas64(B0p + j, old, kv) == old) return kStUpdated;
-                continue;
-            }
-            uint32_t e = empty_mask(B);
-            if (!e) break;
-            if (cas64(B0p + (__ffs(e) - 1), 0ull, kv) == 0ull) return kStInserted;
-        }
-    }
-    return insert_slow<P>(t, k, kv, b0);
+    const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
+    uint8_t st = insert_lockfree<P, kMode>(t, k, kv, b0, b1);
+    if (st) return st;
+    if (kDefer) return kStDefer;
+    return insert_locked_path<P>(t, k, kv, b0, b1);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -65,7 +65,10 @@ struct hive_table {
     uint32_t level = 0;
     void* block = nullptr;   // single allocation holding every array
     size_t block_bytes = 0;
-    u64* scratch = nullptr;  // 8-byte device scratch for size/dump counts
+    u64* scratch = nullptr;  // device words: [0] size/dump count, [1] deferred-op count
+    uint32_t* defer_q = nullptr;  // deferred-op queue (one index per op of the largest batch)
+    uint64_t defer_cap = 0;
+    int num_sms = 148;
 };
 
 namespace {
@@ -94,7 +97,7 @@ Carve carve(uint64_t nb_cap) {
     c.lbits = align256(c.sbits + words * 4);
     c.ctr = align256(c.lbits + words * 4);
     c.scratch = align256(c.ctr + HIVE_NUM_COUNTERS * 8);
-    c.total = align256(c.scratch + 8);
+    c.total = align256(c.scratch + 16);
     return c;
 }
 
@@ -116,16 +119,50 @@ void bind_arrays(hive_table* h, void* block, uint64_t nb_cap) {
 // Kernels
 // ---------------------------------------------------------------------------------------------
 
-template <int P>
+// The queue of ops deferred by a first pass to the second (insert stages C/D): op indices and
+// their count.  q == nullptr disables deferral.
+struct Defer {
+    uint32_t* q;
+    u64* n;
+};
+
+// Appends index i for every lane whose st is kStDefer, one atomic per warp.  Every lane of the
+// warp must call it.
+__device__ __forceinline__ void defer_push(const Defer& d, bool deferred, uint64_t i) {
+    const unsigned m = __ballot_sync(0xffffffffu, deferred);
+    if (!m) return;
+    const unsigned lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    u64 base = 0;
+    if ((int)lane == leader) base = atomicAdd(d.n, (u64)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (deferred) d.q[base + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
+}
+
+// First pass (kDefer) or the whole protocol in one pass (!kDefer, batches too large to queue).
+template <int P, bool kDefer, int kMode>
 __global__ void __launch_bounds__(kBlock) k_insert(hive::Table t, const uint32_t* __restrict__ keys,
                                                    const uint32_t* __restrict__ vals, uint64_t n,
-                                                   uint8_t* __restrict__ status) {
+                                                   uint8_t* __restrict__ status, Defer d) {
     const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t k = __ldcs(keys + i);
-    const uint32_t v = __ldcs(vals + i);
-    const uint8_t st = hive::insert_one<P>(t, k, v);
-    if (status) __stcs(status + i, st);
+    const bool active = i < n;
+    uint8_t st = hive::kStFail;
+    if (active) st = hive::insert_one<P, kDefer, kMode>(t, __ldcs(keys + i), __ldcs(vals + i));
+    if (kDefer) defer_push(d, st == hive::kStDefer, i);
+    if (active && st != hive::kStDefer && status) __stcs(status + i, st);
+}
+
+// Second pass: the deferred inserts, grid-stride over the queue.
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_insert_deferred(hive::Table t, const uint32_t* __restrict__ keys,
+                                                            const uint32_t* __restrict__ vals,
+                                                            uint8_t* __restrict__ status, Defer d) {
+    const u64 cnt = *d.n;
+    for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
+        const uint32_t i = d.q[j];
+        const uint8_t st = hive::insert_one<P>(t, keys[i], vals[i]);
+        if (status) status[i] = st;
+    }
 }
 
 template <int P>
@@ -149,13 +186,13 @@ __global__ void __launch_bounds__(kBlock) k_erase(hive::Table t, const uint32_t*
     if (status) __stcs(status + i, (uint8_t)r);
 }
 
-template <int P>
+template <int P, bool kDefer, int kMode>
 __device__ __forceinline__ uint8_t apply_one(const hive::Table& t, uint8_t type, uint32_t k, uint32_t v,
                                              uint32_t* out) {
     *out = 0;
     switch (type) {
         case HIVE_OP_INSERT:
-            return hive::insert_one<P>(t, k, v);
+            return hive::insert_one<P, kDefer, kMode>(t, k, v);
         case HIVE_OP_LOOKUP: {
             uint32_t fv = 0;
             bool f = hive::find_one<P, false>(t, k, &fv);
@@ -175,31 +212,83 @@ __device__ __forceinline__ uint8_t apply_one(const hive::Table& t, uint8_t type,
     }
 }
 
-template <int P>
+template <int P, bool kDefer, int kMode>
 __global__ void __launch_bounds__(kBlock) k_apply(hive::Table t, const uint8_t* __restrict__ types,
                                                   const uint32_t* __restrict__ keys,
                                                   const uint32_t* __restrict__ vals, uint64_t n,
-                                                  uint8_t* __restrict__ status, uint32_t* __restrict__ outv) {
+                                                  uint8_t* __restrict__ status, uint32_t* __restrict__ outv, Defer d) {
     const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
-    if (i >= n) return;
-    uint32_t o;
-    const uint8_t st = apply_one<P>(t, __ldcs(types + i), __ldcs(keys + i), vals ? __ldcs(vals + i) : 0u, &o);
+    const bool active = i < n;
+    uint32_t o = 0;
+    uint8_t st = 0;
+    if (active)
+        st = apply_one<P, kDefer, kMode>(t, __ldcs(types + i), __ldcs(keys + i), vals ? __ldcs(vals + i) : 0u, &o);
+    if (kDefer) defer_push(d, st == hive::kStDefer, i);
+    if (!active || st == hive::kStDefer) return;
     if (status) __stcs(status + i, st);
     if (outv) __stcs(outv + i, o);
 }
 
-// Reference Operation records: {int32 type; pad; uint64 key} (include/utils.h:18-21).
+// Second pass of k_apply: the deferred inserts (their out value is 0).
 template <int P>
+__global__ void __launch_bounds__(kBlock) k_apply_deferred(hive::Table t, const uint32_t* __restrict__ keys,
+                                                           const uint32_t* __restrict__ vals,
+                                                           uint8_t* __restrict__ status, uint32_t* __restrict__ outv,
+                                                           Defer d) {
+    const u64 cnt = *d.n;
+    for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
+        const uint32_t i = d.q[j];
+        const uint8_t st = hive::insert_one<P>(t, keys[i], vals ? vals[i] : 0u);
+        if (status) status[i] = st;
+        if (outv) outv[i] = 0u;
+    }
+}
+
+// Reference Operation records: {int32 type; pad; uint64 key} (include/utils.h:18-21).
+__device__ __forceinline__ unsigned long long ref_result(uint8_t st) {
+    return (unsigned long long)(st != hive::kStFail && st != hive::kStError);
+}
+
+template <int P, bool kDefer, int kMode>
 __global__ void __launch_bounds__(kBlock) k_apply_ref(hive::Table t, const ulonglong2* __restrict__ ops, uint64_t n,
-                                                      unsigned long long* __restrict__ results) {
+                                                      unsigned long long* __restrict__ results, Defer d) {
+    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < n;
+    uint8_t st = 0;
+    if (active) {
+        const ulonglong2 rec = __ldcs(ops + i);
+        const int32_t type = (int32_t)(uint32_t)rec.x;
+        const uint32_t k = (uint32_t)rec.y;
+        uint32_t o;
+        st = (type >= 0 && type <= 3) ? apply_one<P, kDefer, kMode>(t, (uint8_t)type, k, k + 1u, &o) : 0;
+    }
+    if (kDefer) defer_push(d, st == hive::kStDefer, i);
+    if (active && st != hive::kStDefer && results) __stcs(results + i, ref_result(st));
+}
+
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_apply_ref_deferred(hive::Table t, const ulonglong2* __restrict__ ops,
+                                                               unsigned long long* __restrict__ results, Defer d) {
+    const u64 cnt = *d.n;
+    for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
+        const uint32_t i = d.q[j];
+        const uint32_t k = (uint32_t)ops[i].y;
+        const uint8_t st = hive::insert_one<P>(t, k, k + 1u);
+        if (results) results[i] = ref_result(st);
+    }
+}
+
+// Lookup-only batches of reference records (HIVE_HINT_LOOKUPS_ONLY): read-only load path, as the
+// reference's hive_lookup_kernel (include/hive_kernels.cuh:76-117).
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_apply_ref_ro(hive::Table t, const ulonglong2* __restrict__ ops,
+                                                         uint64_t n, unsigned long long* __restrict__ results) {
     const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
     if (i >= n) return;
     const ulonglong2 rec = __ldcs(ops + i);
-    const int32_t type = (int32_t)(uint32_t)rec.x;
-    const uint32_t k = (uint32_t)rec.y;
-    uint32_t o;
-    uint8_t st = (type >= 0 && type <= 3) ? apply_one<P>(t, (uint8_t)type, k, k + 1u, &o) : 0;
-    if (results) __stcs(results + i, (unsigned long long)(st != hive::kStFail && st != hive::kStError));
+    uint32_t v;
+    const bool f = (int32_t)(uint32_t)rec.x == HIVE_OP_LOOKUP && hive::find_one<P, true>(t, (uint32_t)rec.y, &v);
+    if (results) __stcs(results + i, (unsigned long long)f);
 }
 
 template <int P>
@@ -430,6 +519,29 @@ int reset(hive_table* h, cudaStream_t s) {
 
 bool valid_table(const hive_table* h) { return h && h->block; }
 
+// The deferred-op queue for a batch of n ops; grows (synchronously) to the largest batch seen.
+// Batches of 2^32 ops or more run without deferral.
+int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d) {
+    *d = Defer{nullptr, h->scratch + 1};
+    if (n > 0xFFFFFFFFull) return HIVE_OK;
+    if (n > h->defer_cap) {
+        HIVE_CUDA(cudaDeviceSynchronize());
+        if (h->defer_q) cudaFree(h->defer_q);
+        h->defer_q = nullptr;
+        h->defer_cap = 0;
+        cudaError_t e = cudaMalloc(&h->defer_q, (size_t)n * 4);
+        if (e != cudaSuccess) return cuda_fail(e);
+        h->defer_cap = n;
+    }
+    HIVE_CUDA(cudaMemsetAsync(h->scratch + 1, 0, 8, s));
+    d->q = h->defer_q;
+    return HIVE_OK;
+}
+
+unsigned second_pass_grid(const hive_table* h, uint64_t n) {
+    return (unsigned)std::min<uint64_t>(grid_for(n), (uint64_t)h->num_sms * 4);
+}
+
 int grow_capacity(hive_table* h, uint64_t need_buckets, cudaStream_t s) {
     if (need_buckets <= h->nb_cap) return HIVE_OK;
     uint64_t nb_cap = std::max<uint64_t>(need_buckets, h->nb_cap * 2);
@@ -570,6 +682,8 @@ int hive_create(const hive_config* cfg, hive_table** out) {
     h->device = dev;
     h->policy = cfg->policy;
     h->n0 = (uint32_t)nb;
+    if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || h->num_sms < 1)
+        h->num_sms = 148;
     Carve c = carve(nb_cap);
     void* block = nullptr;
     cudaError_t e = cudaMalloc(&block, c.total);
@@ -599,6 +713,7 @@ int hive_destroy(hive_table* h) {
         DeviceGuard g(h->device);
         cudaError_t e = cudaFree(h->block);
         if (e != cudaSuccess) rc = cuda_fail(e);
+        if (h->defer_q && (e = cudaFree(h->defer_q)) != cudaSuccess) rc = cuda_fail(e);
     }
     delete h;
     return rc;
@@ -621,13 +736,35 @@ int hive_clear(hive_table* h, void* stream) {
         else kern<0><<<grid, block, 0, stream>>>(__VA_ARGS__);                             \
     } while (0)
 
+// Launch a two-pass kernel: the first pass with deferral when the queue exists, else one pass.
+#define HIVE_DISPATCH_D(kern, d, grid, block, stream, ...)                                  \
+    do {                                                                                   \
+        const bool p1_ = h->policy == HIVE_POLICY_MURMURCITYHASH;                          \
+        const bool holes_ = h->t.flags & hive::kFlagHoles;                                 \
+        if (d.q && !holes_) {                                                              \
+            if (p1_) kern<1, true, hive::kModeMono><<<grid, block, 0, stream>>>(__VA_ARGS__);  \
+            else kern<0, true, hive::kModeMono><<<grid, block, 0, stream>>>(__VA_ARGS__);      \
+        } else if (d.q) {                                                                  \
+            if (p1_) kern<1, true, hive::kModeHoles><<<grid, block, 0, stream>>>(__VA_ARGS__); \
+            else kern<0, true, hive::kModeHoles><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
+        } else {                                                                           \
+            if (p1_) kern<1, false, hive::kModeRuntime><<<grid, block, 0, stream>>>(__VA_ARGS__); \
+            else kern<0, false, hive::kModeRuntime><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
+        }                                                                                  \
+    } while (0)
+
 int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uint64_t n, uint8_t* status,
                 void* stream) {
     if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
     if (n == 0) return HIVE_OK;
     if (!keys || !values) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
-    HIVE_DISPATCH(k_insert, grid_for(n), kBlock, (cudaStream_t)stream, h->t, keys, values, n, status);
+    cudaStream_t s = (cudaStream_t)stream;
+    Defer d;
+    int rc = prepare_defer(h, n, s, &d);
+    if (rc) return rc;
+    HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, n, status, d);
+    if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, d);
     return launch_check();
 }
 
@@ -656,9 +793,14 @@ int hive_apply_ops(hive_table* h, const uint8_t* types, const uint32_t* keys, co
     if (n == 0) return HIVE_OK;
     if (!types || !keys) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
     if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
-    HIVE_DISPATCH(k_apply, grid_for(n), kBlock, (cudaStream_t)stream, h->t, types, keys, values, n, status,
-                  out_values);
+    Defer d;
+    int rc = prepare_defer(h, n, s, &d);
+    if (rc) return rc;
+    HIVE_DISPATCH_D(k_apply, d, grid_for(n), kBlock, s, h->t, types, keys, values, n, status, out_values, d);
+    if (d.q)
+        HIVE_DISPATCH(k_apply_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, out_values, d);
     return launch_check();
 }
 
@@ -668,9 +810,21 @@ int hive_apply_reference_ops(hive_table* h, const void* ops, uint64_t n, uint64_
     if (n == 0) return HIVE_OK;
     if (!ops || ((uintptr_t)ops & 15)) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
+    if (hints & HIVE_HINT_LOOKUPS_ONLY) {
+        HIVE_DISPATCH(k_apply_ref_ro, grid_for(n), kBlock, (cudaStream_t)stream, h->t, (const ulonglong2*)ops, n,
+                      (unsigned long long*)results);
+        return launch_check();
+    }
+    cudaStream_t s = (cudaStream_t)stream;
     if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
-    HIVE_DISPATCH(k_apply_ref, grid_for(n), kBlock, (cudaStream_t)stream, h->t, (const ulonglong2*)ops, n,
-                  (unsigned long long*)results);
+    Defer d;
+    int rc = prepare_defer(h, n, s, &d);
+    if (rc) return rc;
+    HIVE_DISPATCH_D(k_apply_ref, d, grid_for(n), kBlock, s, h->t, (const ulonglong2*)ops, n,
+                    (unsigned long long*)results, d);
+    if (d.q)
+        HIVE_DISPATCH(k_apply_ref_deferred, second_pass_grid(h, n), kBlock, s, h->t, (const ulonglong2*)ops,
+                      (unsigned long long*)results, d);
     return launch_check();
 }
 

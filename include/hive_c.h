@@ -58,7 +58,10 @@ extern "C" {
 #define HIVE_OP_NONE 4
 
 /* hints for hive_apply_ops / hive_apply_reference_ops */
-#define HIVE_HINT_NO_DELETES 1u /* caller guarantees the batch holds no DELETE op */
+#define HIVE_HINT_NO_DELETES 1u   /* caller guarantees the batch holds no DELETE op                */
+#define HIVE_HINT_LOOKUPS_ONLY 2u /* batch holds only LOOKUP/NONE ops and no other call modifies the
+                                     table meanwhile: lookups take the read-only load path and any
+                                     other op type is answered 0 without running               */
 
 /* ---- counters (hive_counters) ---------------------------------------------------------------- */
 #define HIVE_CTR_SLOW_PATH 0    /* inserts whose canonical bucket was full                     */

@@ -81,8 +81,49 @@ def build_reference_pins(force: bool = False) -> list[Path]:
     return outs
 
 
+DROPIN_DRIVERS = {
+    "dropin_hive_table_benchmark": "benchmark/hive_table_benchmark.cpp",
+    "dropin_hive_lookup_only_benchmark": "benchmark/hive_lookup_only_benchmark.cpp",
+    "dropin_ycsb_benchmark": "benchmark/ycsb_benchmark.cpp",
+}
+
+
+def build_dropin_drivers(force: bool = False) -> list[Path]:
+    """The reference's own CLI drivers and workload harness (benchmark/*.cpp,
+    src/hashTableBenchmark.cc, src/GPUTimer.cc), unchanged, compiled against this repository's
+    include/hive_hash_table.cuh and linked to libhive_compat.so + libhive_b200.so instead of the
+    reference's src/hive_dispatch.cu and src/hive_memory.cu.  Demonstrates the drop-in boundary."""
+    if not reference_available():
+        return []
+    repo = HERE.parent
+    pkg_lib = repo / "hivehashtable_b200" / "lib"
+    if str(repo) not in sys.path:
+        sys.path.insert(0, str(repo))
+    from hivehashtable_b200 import build as pbuild
+
+    pbuild.build_core()
+    pbuild.build_compat()
+    REF_OUT.mkdir(exist_ok=True)
+    cccl = Path(_nvcc()).resolve().parent.parent / "include" / "cccl"
+    common = [REFERENCE_ROOT / "src" / "hashTableBenchmark.cc", REFERENCE_ROOT / "src" / "GPUTimer.cc"]
+    outs = []
+    for name, drv in DROPIN_DRIVERS.items():
+        o = REF_OUT / name
+        deps = [REFERENCE_ROOT / drv, *common, repo / "include" / "hive_hash_table.cuh", pkg_lib / "libhive_compat.so"]
+        if force or _stale(o, deps):
+            cmd = [_nvcc(), *ARCH, "-std=c++17", "-O2", f"-I{repo / 'include'}", f"-I{REFERENCE_ROOT / 'include'}",
+                   f"-I{cccl}"]
+            for src in [REFERENCE_ROOT / drv, *common]:
+                cmd += ["-x", "cu", src]
+            cmd += ["-o", o, f"-L{pkg_lib}", "-lhive_compat", "-lhive_b200", f"-Xlinker=-rpath={pkg_lib}",
+                    "-Xlinker=-rpath=$ORIGIN/../../hivehashtable_b200/lib", "-lcudart"]
+            _run(cmd)
+        outs.append(o)
+    return outs
+
+
 def build_all(force: bool = False) -> list[Path]:
-    return [build_oracle(force), *build_reference_pins(force)]
+    return [build_oracle(force), *build_reference_pins(force), *build_dropin_drivers(force)]
 
 
 if __name__ == "__main__":
