@@ -57,6 +57,7 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-probe", action="store_true", help="skip the random-bucket ceiling probes")
     ap.add_argument("--cpu-sample-log", type=int, default=24, help="log2 slots of the CPU-baseline sample")
     return ap.parse_args()
 
@@ -110,6 +111,46 @@ class ClockSampler:
         reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(sm)}
+
+
+def random_bucket_ceiling(dev, table_bytes):
+    """Throughput of the table's raw access patterns with nothing else in the kernel
+    (hivehashtable_b200/csrc/hive_probe.cu): random 64 B bucket reads over a 4 GiB buffer, over a
+    buffer the size of the table, over a 32 MiB L2-resident buffer; read + 8 B CAS; two dependent
+    reads.  GB/s counts 64 B per bucket read and 32 B per CAS'd sector."""
+    import ctypes
+    import torch
+    from hivehashtable_b200 import build as pbuild
+
+    lib = ctypes.CDLL(str(pbuild.LIB / "libhive_probe.so"))
+    f = lib.hive_probe_random_buckets
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64,
+                  ctypes.c_void_p, ctypes.c_void_p]
+    sink = torch.zeros(1, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    n = 1 << 26
+    out = {}
+    cases = [("read64_4GiB", 4 << 30, 0, 64), ("read64_table", table_bytes, 0, 64),
+             ("read64_cas_table", table_bytes, 1, 96), ("read64x2_table", table_bytes, 2, 128),
+             ("read64_32MiB_l2", 32 << 20, 0, 64)]
+    for name, size, mode, bpo in cases:
+        buf = torch.zeros(size // 8, dtype=torch.int64, device=dev)
+        nb = size // 64
+        for _ in range(2):
+            assert f(buf.data_ptr(), nb, n, mode, 1, sink.data_ptr(), stream.cuda_stream) == 0
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        a.record(stream)
+        for r in range(reps):
+            f(buf.data_ptr(), nb, n, mode, 7 + r, sink.data_ptr(), stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / reps
+        out[name] = {"gbs": round(n * bpo / (ms / 1e3) / 1e9, 1), "gops": round(n / (ms / 1e3) / 1e9, 2)}
+        del buf
+    torch.cuda.empty_cache()
+    return out
 
 
 def cpu_baseline(args, threads=None):
@@ -302,6 +343,9 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(args)
+    ceiling = None
+    if rank == 0 and not args.no_probe:
+        ceiling = random_bucket_ceiling(dev, cap * 8)
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -320,6 +364,14 @@ def main():
                         "frac": round(ach / peak, 4), "traffic": tr, "peak_kind": peak_kind,
                         "algorithmic_bytes": kd["bytes"], "ms_per_launch": round(kd["ms"], 4),
                         "mops": round(kd["ops"] / kd["ms"] / 1e3, 1)}
+        if ceiling:
+            # the same ops at the probe's raw access rate: insert = one bucket read + CAS;
+            # lookup = one read when present, two dependent reads when absent
+            ins_ceiling = ceiling["read64_cas_table"]["gops"]
+            p = args.present
+            look_ceiling = 1.0 / (p / ceiling["read64_table"]["gops"] + (1 - p) / ceiling["read64x2_table"]["gops"])
+            rl["k_insert"]["frac_of_probe_ops"] = round(rl["k_insert"]["mops"] / 1e3 / ins_ceiling, 4)
+            rl["k_find"]["frac_of_probe_ops"] = round(rl["k_find"]["mops"] / 1e3 / look_ceiling, 4)
         dom = max(kernels, key=lambda k: kernels[k]["ms"])
         roof = dict(rl[dom], kernel=dom)
         line = {"metric": METRIC, "value": round(2 * n * args.steps * world / (ms / 1e3) / 1e6, 2), "unit": UNIT,
@@ -329,7 +381,7 @@ def main():
                 "config": workload_config(args, world), "roofline": roof, "roofline_all": rl,
                 "insert_mops": rl["k_insert"]["mops"], "lookup_mops": rl["k_find"]["mops"],
                 "e2e": e2e, "cpu_baseline": cb, "gpu_launches": 4 * args.steps,
-                "insert_counters": step_counters,
+                "insert_counters": step_counters, "random_bucket_ceiling": ceiling,
                 "clocks": sampler.summary()}
         print(json.dumps(line), flush=True)
     table.close()

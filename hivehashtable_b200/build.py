@@ -80,8 +80,18 @@ def build_compat(force: bool = False) -> Path:
     return out
 
 
+def build_probe(force: bool = False) -> Path:
+    out = LIB / "libhive_probe.so"
+    src = CSRC / "hive_probe.cu"
+    if force or _stale(out, [src]):
+        LIB.mkdir(exist_ok=True)
+        _run([_nvcc(), *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-fvisibility=hidden", str(src), "-o", str(out), "-lcudart"])
+    return out
+
+
 def build_all(force: bool = False) -> list[Path]:
-    outs = [build_core(force), build_workload(force)]
+    outs = [build_core(force), build_workload(force), build_probe(force)]
     if (CSRC / "hive_compat.cpp").exists():
         outs.append(build_compat(force))
     return outs

@@ -1,0 +1,89 @@
+// hive_probe.cu -- random-bucket bandwidth probes for the roofline of the Hive kernels.
+//
+// The table's hot loop is a random 64 B bucket read (two 32 B sectors) followed, for an insert,
+// by an 8 B CAS into that bucket.  These probes time exactly those access patterns over a buffer
+// of the caller's size with no hashing, matching or control flow, so their throughput is the
+// ceiling the table kernels are measured against (the plain copy bandwidth is not: sequential
+// streams keep every DRAM page open, random 64 B reads do not).
+//
+//   mode 0  read one random 64 B bucket per thread
+//   mode 1  read one random 64 B bucket, then CAS 8 B in it (value unchanged)
+//   mode 2  read two random 64 B buckets per thread (dependent: the second address comes from the
+//           first bucket's contents), the absent-key lookup pattern
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace {
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+__device__ __forceinline__ void ld64(const unsigned long long* p, unsigned long long (&v)[8]) {
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(v[0]), "=l"(v[1]), "=l"(v[2]), "=l"(v[3]) : "l"(p));
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(v[4]), "=l"(v[5]), "=l"(v[6]), "=l"(v[7]) : "l"(p + 4));
+}
+
+__device__ __forceinline__ void ld64_relaxed(const unsigned long long* p, unsigned long long (&v)[8]) {
+    asm volatile("ld.relaxed.gpu.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(v[0]), "=l"(v[1]), "=l"(v[2]), "=l"(v[3]) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(v[4]), "=l"(v[5]), "=l"(v[6]), "=l"(v[7]) : "l"(p + 4) : "memory");
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(256) k_probe(unsigned long long* buf, uint64_t nb, uint64_t n, uint64_t seed,
+                                               unsigned long long* sink) {
+    const uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t b = mix64(i ^ seed) % nb;
+    unsigned long long v[8];
+    unsigned long long acc;
+    if (kMode == 1) {
+        ld64_relaxed(buf + b * 8, v);
+        const int j = (int)(i & 7);
+        unsigned long long cur = v[0];
+#pragma unroll
+        for (int q = 1; q < 8; ++q)
+            if (q == j) cur = v[q];
+        acc = atomicCAS(buf + b * 8 + j, cur, cur);
+    } else {
+        ld64(buf + b * 8, v);
+        acc = v[0] ^ v[1] ^ v[2] ^ v[3] ^ v[4] ^ v[5] ^ v[6] ^ v[7];
+        if (kMode == 2) {
+            const uint64_t b2 = mix64(acc ^ i) % nb;
+            ld64(buf + b2 * 8, v);
+            acc ^= v[0] ^ v[1] ^ v[2] ^ v[3] ^ v[4] ^ v[5] ^ v[6] ^ v[7];
+        }
+    }
+    if (acc == 0x9e3779b97f4a7c15ull) *sink = acc;  // keeps the loads live; practically never taken
+}
+
+}  // namespace
+
+extern "C" {
+
+// buf: device buffer of nb 64-byte buckets; n: buckets read (threads).  Returns a cudaError_t.
+__attribute__((visibility("default"))) int hive_probe_random_buckets(void* buf, uint64_t nb, uint64_t n, int mode,
+                                                                      uint64_t seed, void* sink, void* stream) {
+    if (!buf || !nb || !sink || mode < 0 || mode > 2) return (int)cudaErrorInvalidValue;
+    if (!n) return 0;
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    cudaStream_t s = (cudaStream_t)stream;
+    auto* p = (unsigned long long*)buf;
+    auto* k = (unsigned long long*)sink;
+    if (mode == 0) k_probe<0><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else if (mode == 1) k_probe<1><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else k_probe<2><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    return (int)cudaGetLastError();
+}
+
+}  // extern "C"
