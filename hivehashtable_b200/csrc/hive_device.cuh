@@ -13,6 +13,11 @@
 //                                it L2-resident (1 MiB at 2^23 buckets)
 //   lock_bits  u32[nb_cap / 32]  eviction locks, 1 bit per bucket (the reference uses a u32
 //                                word per bucket, include/hive_hash_table_struct.cuh:101-117)
+//   full_bits  u32[nb_cap / 32]  bit b set = bucket b was seen full (set by the claim that took
+//                                its last free slot, cleared by deletes).  A hint only: the
+//                                evictor reads it for all 8 victims' alternate buckets at once
+//                                (L2 hits) and then reads just one bucket that has room, where
+//                                the reference probes victims' buckets one by one
 //   counters   u64[16]           slow-path event counters and the sticky error word
 //
 // A slot holds (value << 32) | key (include/hive_hash_table_struct.cuh:297-311); key 0 is the
@@ -65,6 +70,7 @@ struct Table {
     u64* stash;
     uint32_t* stash_bits;
     uint32_t* lock_bits;
+    uint32_t* full_bits;
     u64* counters;
     u64 m_lo;  // fastmod magic for n_lo
     u64 m_hi;  // fastmod magic for 2 * n_lo
@@ -237,19 +243,36 @@ __device__ __forceinline__ bool stash_flag_ro(const Table& t, uint32_t b) {
 __device__ __forceinline__ void count(const Table& t, int ctr) { atomicAdd(t.counters + ctr, 1ull); }
 __device__ __forceinline__ void raise_error(const Table& t, u64 bits) { atomicOr(t.counters + kCtrError, bits); }
 
+// Full-bucket hints.  mark_full is called by the claim that took a bucket's last free slot.
+__device__ __forceinline__ void mark_full(const Table& t, uint32_t b) {
+    asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(t.full_bits + (b >> 5)), "r"(1u << (b & 31))
+                 : "memory");
+}
+__device__ __forceinline__ void mark_not_full(const Table& t, uint32_t b) {
+    asm volatile("red.relaxed.gpu.global.and.b32 [%0], %1;" ::"l"(t.full_bits + (b >> 5)), "r"(~(1u << (b & 31)))
+                 : "memory");
+}
+__device__ __forceinline__ bool full_flag(const Table& t, uint32_t b) {
+    return (ld_relaxed_u32(t.full_bits + (b >> 5)) >> (b & 31)) & 1u;
+}
+
+// Release/acquire-ordered fence for the publication steps below (cheaper than __threadfence,
+// which is sequentially consistent).
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 constexpr int kRetryLimit = 64;       // CAS retries of one op on one bucket
 constexpr int kLockSpinLimit = 1 << 16;  // lock attempts before the wait is declared expired
 
-// Bounded test-and-set on the bucket's lock bit.  Returns false when the wait expired.
+// Bounded test-and-set on the bucket's lock bit with acquire semantics.  Returns false when the
+// wait expired.
 __device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
     uint32_t* w = t.lock_bits + (b >> 5);
     const uint32_t bit = 1u << (b & 31);
     unsigned ns = 32;
     for (int i = 0; i < kLockSpinLimit; ++i) {
-        if (!(atomicOr(w, bit) & bit)) {
-            __threadfence();
-            return true;
-        }
+        uint32_t old;
+        asm volatile("atom.acquire.gpu.global.or.b32 %0, [%1], %2;" : "=r"(old) : "l"(w), "r"(bit) : "memory");
+        if (!(old & bit)) return true;
         __nanosleep(ns);
         if (ns < 1024) ns <<= 1;
     }
@@ -258,8 +281,8 @@ __device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
     return false;
 }
 __device__ __forceinline__ void unlock_bucket(const Table& t, uint32_t b) {
-    __threadfence();
-    atomicAnd(t.lock_bits + (b >> 5), ~(1u << (b & 31)));
+    asm volatile("red.release.gpu.global.and.b32 [%0], %1;" ::"l"(t.lock_bits + (b >> 5)), "r"(~(1u << (b & 31)))
+                 : "memory");
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -375,23 +398,50 @@ enum { kEvPlaced = 1, kEvRetry = 2, kEvNone = 0 };
 template <int P>
 __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket& B0, uint32_t b0, u64 kv) {
     const int limit = t.max_evictions < (uint32_t)kSlots ? (int)t.max_evictions : kSlots;
-    for (int j = 0; j < limit; ++j) {
-        u64 vkv = slot_at(B0, j);
-        if (vkv == 0ull) {
-            // A slot freed up (delete) since the bucket was read.
-            return cas64(B0p + j, 0ull, kv) == 0ull ? kEvPlaced : kEvRetry;
-        }
+    // Candidate victims: slots j < limit (the reference's kick % 8 order) whose key lives in its
+    // own H0 (= b0) and whose H1 is another bucket.  A slot that freed up is taken directly.
+    uint32_t alts[kSlots];
+    uint32_t cand = 0;
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j) {
+        alts[j] = b0;
+        if (j >= limit) continue;
+        const u64 vkv = B0.s[j];
+        if (vkv == 0ull) return cas64(B0p + j, 0ull, kv) == 0ull ? kEvPlaced : kEvRetry;
         const uint32_t vk = key_of(vkv);
         if (bucket_addr(t, Policy<P>::h0(vk)) != b0) continue;  // victim lives in its H1
         const uint32_t alt = bucket_addr(t, Policy<P>::h1(vk));
         if (alt == b0) continue;
+        alts[j] = alt;
+        cand |= 1u << j;
+    }
+    // One round of independent L2 reads of the candidates' full bits instead of a chain of
+    // bucket reads; only buckets not known to be full are read.
+    uint32_t open = 0;
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j)
+        if ((cand >> j) & 1u)
+            if (!((__ldcg(t.full_bits + (alts[j] >> 5)) >> (alts[j] & 31)) & 1u)) open |= 1u << j;
+    while (open) {
+        const int j = __ffs(open) - 1;
+        open &= open - 1;
+        u64 vkv = slot_at(B0, j);
+        const uint32_t vk = key_of(vkv);
+        uint32_t alt = alts[0];
+#pragma unroll
+        for (int q = 1; q < kSlots; ++q)
+            if (q == j) alt = alts[q];
         u64* Ap = t.slots + (size_t)alt * kSlots;
         Bucket A;
         load_bucket(Ap, A);
-        uint32_t e = empty_mask(A);
-        if (!e) continue;
+        const uint32_t e = empty_mask(A);
+        if (!e) {
+            mark_full(t, alt);
+            continue;
+        }
         const int d = __ffs(e) - 1;
         if (cas64(Ap + d, 0ull, vkv) != 0ull) continue;  // lost the free slot; next victim
+        if (__popc(e) == 1) mark_full(t, alt);
         // The victim is now visible in both H0 slot j and H1 slot d.
         for (int r = 0; r < kRetryLimit; ++r) {
             u64 obs = cas64(B0p + j, vkv, kv);
@@ -401,7 +451,7 @@ __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket&
             }
             if (obs == 0ull) {
                 // Victim deleted meanwhile: drop the copy unless it changed, take the free slot.
-                cas64(Ap + d, vkv, 0ull);
+                if (cas64(Ap + d, vkv, 0ull) == vkv) mark_not_full(t, alt);
                 return cas64(B0p + j, 0ull, kv) == 0ull ? kEvPlaced : kEvRetry;
             }
             if (key_of(obs) == vk) {
@@ -410,7 +460,7 @@ __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket&
                 vkv = obs;
                 continue;
             }
-            cas64(Ap + d, vkv, 0ull);
+            if (cas64(Ap + d, vkv, 0ull) == vkv) mark_not_full(t, alt);
             return kEvRetry;
         }
         count(t, kCtrRetryOut);
@@ -454,6 +504,7 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         if (e) {
             int j = __ffs(e) - 1;
             if (cas64(B0p + j, 0ull, kv) == 0ull) {
+                if (__popc(e) == 1) mark_full(t, b0);
                 if (holes && resolve_duplicate(t, B0p, k, j, kv)) return kStUpdated;
                 return kStInserted;
             }
@@ -463,6 +514,7 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         if (e) {
             int j = __ffs(e) - 1;
             if (cas64(B1p + j, 0ull, kv) == 0ull) {
+                if (__popc(e) == 1) mark_full(t, b1);
                 if (holes && resolve_duplicate(t, B1p, k, j, kv)) return kStUpdated;
                 return kStInserted;
             }
@@ -474,7 +526,7 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         // Stage D: the canonical bucket's stash.  Its flag is raised before the entry is
         // written, so a reader that finds the entry also finds the flag set.
         atomicOr(t.stash_bits + (b0 >> 5), 1u << (b0 & 31));
-        __threadfence();
+        fence_acq_rel();
         for (int q = 0; q < kRetryLimit; ++q) {
             Bucket S;
             load_bucket(Sp, S);
@@ -498,7 +550,8 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
 
 // Without holes: update k in bucket p or claim p's lowest free slot.  Returns kStUpdated /
 // kStInserted, or 0 when p is full (or its retry budget ran out: the locked path finishes).
-__device__ __forceinline__ uint8_t claim_or_update(u64* p, uint32_t k, u64 kv) {
+__device__ __forceinline__ uint8_t claim_or_update(const Table& t, uint32_t b, uint32_t k, u64 kv) {
+    u64* p = t.slots + (size_t)b * kSlots;
     for (int r = 0; r < kRetryLimit; ++r) {
         Bucket B;
         load_bucket(p, B);
@@ -511,7 +564,10 @@ __device__ __forceinline__ uint8_t claim_or_update(u64* p, uint32_t k, u64 kv) {
         }
         uint32_t e = empty_mask(B);
         if (!e) return 0;
-        if (cas64(p + (__ffs(e) - 1), 0ull, kv) == 0ull) return kStInserted;
+        if (cas64(p + (__ffs(e) - 1), 0ull, kv) == 0ull) {
+            if (__popc(e) == 1) mark_full(t, b);
+            return kStInserted;
+        }
     }
     return 0;
 }
@@ -528,9 +584,9 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
     u64* B1p = t.slots + (size_t)b1 * kSlots;
     const bool holes = kMode == kModeHoles || (kMode == kModeRuntime && (t.flags & kFlagHoles));
     if (!holes) {
-        uint8_t st = claim_or_update(B0p, k, kv);
+        uint8_t st = claim_or_update(t, b0, k, kv);
         if (st || b1 == b0) return st;
-        return claim_or_update(B1p, k, kv);
+        return claim_or_update(t, b1, k, kv);
     }
     // With holes a key may sit in H1 or the stash while H0 has room: scan all three first.
     u64* Sp = t.stash + (size_t)b0 * kSlots;
@@ -559,13 +615,18 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
         }
         uint32_t e = empty_mask(B0);
         u64* Cp = B0p;
+        uint32_t cb = b0;
         if (!e && b1 != b0) {
             e = empty_mask(B1);
             Cp = B1p;
+            cb = b1;
         }
         if (!e) return 0;
         int j = __ffs(e) - 1;
-        if (cas64(Cp + j, 0ull, kv) == 0ull) return resolve_duplicate(t, Cp, k, j, kv) ? kStUpdated : kStInserted;
+        if (cas64(Cp + j, 0ull, kv) == 0ull) {
+            if (__popc(e) == 1) mark_full(t, cb);
+            return resolve_duplicate(t, Cp, k, j, kv) ? kStUpdated : kStInserted;
+        }
     }
     return 0;
 }
@@ -598,17 +659,23 @@ __device__ __forceinline__ uint8_t insert_one(const Table& t, uint32_t k, uint32
 // Delete: remove every copy in H0, H1 and the canonical stash, no early exit
 // (include/hive_hash_delete.cuh:168-194).  Returns true if any copy was removed.
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ bool erase_in(const Table& t, u64* p, uint32_t k) {
+// Removes every copy of k from bucket p.  is_slots: p is table bucket b (not a stash), whose
+// full hint is cleared after a removal.
+__device__ __forceinline__ bool erase_in(const Table& t, u64* p, uint32_t k, bool is_slots, uint32_t b) {
     bool removed = false;
     for (int r = 0; r < kRetryLimit; ++r) {
         Bucket B;
         load_bucket(p, B);
         uint32_t m = match_mask(B, k);
-        if (!m) return removed;
+        if (!m) {
+            if (removed && is_slots) mark_not_full(t, b);
+            return removed;
+        }
         int j = __ffs(m) - 1;
         u64 old = slot_at(B, j);
         if (cas64(p + j, old, 0ull) == old) removed = true;
     }
+    if (removed && is_slots) mark_not_full(t, b);
     count(t, kCtrRetryOut);
     raise_error(t, kErrRetryOut);
     return removed;
@@ -619,9 +686,9 @@ __device__ __forceinline__ bool erase_one(const Table& t, uint32_t k) {
     if (k == 0) return false;
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
     const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
-    bool removed = erase_in(t, t.slots + (size_t)b0 * kSlots, k);
-    if (b1 != b0) removed |= erase_in(t, t.slots + (size_t)b1 * kSlots, k);
-    if (stash_flag(t, b0)) removed |= erase_in(t, t.stash + (size_t)b0 * kSlots, k);
+    bool removed = erase_in(t, t.slots + (size_t)b0 * kSlots, k, true, b0);
+    if (b1 != b0) removed |= erase_in(t, t.slots + (size_t)b1 * kSlots, k, true, b1);
+    if (stash_flag(t, b0)) removed |= erase_in(t, t.stash + (size_t)b0 * kSlots, k, false, b0);
     return removed;
 }
 

@@ -86,7 +86,7 @@ void set_geometry(hive_table* h, uint32_t level, uint32_t split) {
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Carve {
-    size_t slots, stash, sbits, lbits, ctr, scratch, total;
+    size_t slots, stash, sbits, lbits, fbits, ctr, scratch, total;
 };
 Carve carve(uint64_t nb_cap) {
     Carve c;
@@ -95,7 +95,8 @@ Carve carve(uint64_t nb_cap) {
     c.stash = align256(c.slots + (size_t)nb_cap * 64);
     c.sbits = align256(c.stash + (size_t)nb_cap * 64);
     c.lbits = align256(c.sbits + words * 4);
-    c.ctr = align256(c.lbits + words * 4);
+    c.fbits = align256(c.lbits + words * 4);
+    c.ctr = align256(c.fbits + words * 4);
     c.scratch = align256(c.ctr + HIVE_NUM_COUNTERS * 8);
     c.total = align256(c.scratch + 16);
     return c;
@@ -111,6 +112,7 @@ void bind_arrays(hive_table* h, void* block, uint64_t nb_cap) {
     h->t.stash = (u64*)(base + c.stash);
     h->t.stash_bits = (uint32_t*)(base + c.sbits);
     h->t.lock_bits = (uint32_t*)(base + c.lbits);
+    h->t.full_bits = (uint32_t*)(base + c.fbits);
     h->t.counters = (u64*)(base + c.ctr);
     h->scratch = (u64*)(base + c.scratch);
 }
@@ -141,7 +143,7 @@ __device__ __forceinline__ void defer_push(const Defer& d, bool deferred, uint64
 
 // First pass (kDefer) or the whole protocol in one pass (!kDefer, batches too large to queue).
 template <int P, bool kDefer, int kMode>
-__global__ void __launch_bounds__(kBlock) k_insert(hive::Table t, const uint32_t* __restrict__ keys,
+__global__ void __launch_bounds__(kBlock, (kDefer && kMode == hive::kModeMono) ? 8 : 1) k_insert(hive::Table t, const uint32_t* __restrict__ keys,
                                                    const uint32_t* __restrict__ vals, uint64_t n,
                                                    uint8_t* __restrict__ status, Defer d) {
     const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
@@ -454,6 +456,9 @@ __global__ void k_split(hive::Table told, hive::Table tnew, uint32_t s, uint32_t
         if (!keep_s) atomicAnd(told.stash_bits + (b >> 5), ~(1u << (b & 31)));
         if (moved_s) atomicOr(told.stash_bits + (nbk >> 5), 1u << (nbk & 31));
     }
+    if (nk == hive::kSlots) hive::mark_full(told, b);
+    else hive::mark_not_full(told, b);
+    if (nd == hive::kSlots) hive::mark_full(told, nbk);
 }
 
 // told: geometry before (buckets [lo, lo + cnt) + n_lo are folded); tnew: after.
@@ -483,6 +488,10 @@ __global__ void k_merge(hive::Table told, hive::Table tnew, uint32_t lo, uint32_
         }
     }
     if (has_stash) atomicAnd(told.stash_bits + (src_b >> 5), ~(1u << (src_b & 31)));
+    hive::mark_not_full(told, src_b);
+    hive::Bucket D;
+    hive::load_bucket(tnew.slots + (size_t)b * hive::kSlots, D);
+    if (!hive::empty_mask(D)) hive::mark_full(told, b);
 }
 
 // Re-insert overflow entries produced by k_merge through the normal insert protocol.
@@ -513,6 +522,7 @@ int reset(hive_table* h, cudaStream_t s) {
     if (rc) return rc;
     HIVE_CUDA(cudaMemsetAsync(h->t.stash_bits, 0, (size_t)words * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.lock_bits, 0, (size_t)words * 4, s));
+    HIVE_CUDA(cudaMemsetAsync(h->t.full_bits, 0, (size_t)words * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.counters, 0, HIVE_NUM_COUNTERS * 8, s));
     return HIVE_OK;
 }
@@ -561,6 +571,8 @@ int grow_capacity(hive_table* h, uint64_t need_buckets, cudaStream_t s) {
         (e = cudaMemcpyAsync(nbase + c.stash, obase + oc.stash, (size_t)nb * 64, cudaMemcpyDeviceToDevice, s)) !=
             cudaSuccess ||
         (e = cudaMemcpyAsync(nbase + c.sbits, obase + oc.sbits, owords * 4, cudaMemcpyDeviceToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(nbase + c.fbits, obase + oc.fbits, owords * 4, cudaMemcpyDeviceToDevice, s)) !=
             cudaSuccess ||
         (e = cudaMemcpyAsync(nbase + c.ctr, obase + oc.ctr, HIVE_NUM_COUNTERS * 8, cudaMemcpyDeviceToDevice, s)) !=
             cudaSuccess ||

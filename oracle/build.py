@@ -81,6 +81,27 @@ def build_reference_pins(force: bool = False) -> list[Path]:
     return outs
 
 
+def build_reference_gpu(force: bool = False) -> list[Path]:
+    """The reference's own GPU path (src/hive_dispatch.cu, src/hive_memory.cu, src/GPUTimer.cc,
+    unchanged, with its include/ tree) for sm_100a, plus the extern "C" harness ref/ref_ab.cu, into
+    oracle/_ref/libhive_ref_gpu.so.  Flags follow the reference Makefile's release build
+    (Makefile:7-13, :33-39): -O3 -lineinfo --extended-lambda."""
+    if not reference_available():
+        return []
+    REF_OUT.mkdir(exist_ok=True)
+    o = REF_OUT / "libhive_ref_gpu.so"
+    srcs = [REFERENCE_ROOT / "src" / "hive_dispatch.cu", REFERENCE_ROOT / "src" / "hive_memory.cu",
+            REFERENCE_ROOT / "src" / "GPUTimer.cc", HERE / "ref" / "ref_ab.cu"]
+    cccl = Path(_nvcc()).resolve().parent.parent / "include" / "cccl"
+    if force or _stale(o, srcs):
+        cmd = [_nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "--extended-lambda", "-shared", "-Xcompiler",
+               "-fPIC", f"-I{REFERENCE_ROOT}", f"-I{REFERENCE_ROOT / 'include'}", f"-I{cccl}"]
+        for s in srcs:
+            cmd += ["-x", "cu", s]
+        _run(cmd + ["-o", o, "-lcudart"])
+    return [o]
+
+
 DROPIN_DRIVERS = {
     "dropin_hive_table_benchmark": "benchmark/hive_table_benchmark.cpp",
     "dropin_hive_lookup_only_benchmark": "benchmark/hive_lookup_only_benchmark.cpp",
@@ -123,7 +144,8 @@ def build_dropin_drivers(force: bool = False) -> list[Path]:
 
 
 def build_all(force: bool = False) -> list[Path]:
-    return [build_oracle(force), *build_reference_pins(force), *build_dropin_drivers(force)]
+    return [build_oracle(force), *build_reference_pins(force), *build_reference_gpu(force),
+            *build_dropin_drivers(force)]
 
 
 if __name__ == "__main__":

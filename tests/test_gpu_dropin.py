@@ -34,12 +34,13 @@ def test_table_benchmark_all_inserts(cuda):
 
 
 def test_table_benchmark_mixed_defaults(cuda):
-    # the driver's default 50/40/10 mix over "uniform" keys (with repeats); lookups and deletes
-    # target inserted keys, so with one iteration after a clear every op type succeeds in part
+    # the driver's default 50/40/10 mix over "uniform" keys (with repeats), timed after a clear:
+    # lookups and deletes race with the inserts of their keys in the same launch, and ops within
+    # one launch are unordered (as in the reference), so only the inserts have a fixed outcome
+    n = int(0.9 * (1 << 16))
     out = _run("dropin_hive_table_benchmark", "--table_size", 16, "--load_factor", 0.9, "--num_iterations", 1,
                "--hash_policy", "MurmurCityHash")
-    assert _count(out, "Successful Inserts")[-1] > 0
-    assert _count(out, "Successful Lookups")[-1] > 0
+    assert _count(out, "Successful Inserts")[-1] == int(n * 0.5)
     assert "Average Time over 1 iterations" in out
 
 
