@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "hive_c.h"
@@ -665,6 +666,7 @@ const char* hive_strerror(int status) {
         case HIVE_ERR_RETRY_LIMIT: return "CAS retry budget ran out inside a kernel";
         case HIVE_ERR_CAPACITY: return "capacity exceeded";
         case HIVE_ERR_NO_DEVICE: return "no usable CUDA device";
+        case HIVE_ERR_TOO_LARGE: return "batch larger than HIVE_NOALLOC_MAX_OPS";
         default: return "unknown status";
     }
 }
@@ -777,6 +779,58 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
     if (rc) return rc;
     HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, n, status, d);
     if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, d);
+    return launch_check();
+}
+
+}  // extern "C"
+
+// ---- hive_insert_noalloc: the second-pass queue in static device memory -------------------------
+// Layout: bytes [0, 8) the queue count, [256, 256 + 4 * HIVE_NOALLOC_MAX_OPS) the op indices.
+// Every device that loads this library holds the array until the process exits.  In host code
+// the name g_noalloc_queue is a host-side stand-in, not a device address: a kernel given it
+// would fault (or, where the GPU can reach host memory, silently use the wrong memory), so the
+// device address is looked up per device with cudaGetSymbolAddress and cached.
+namespace {
+constexpr size_t kNoAllocHeaderWords = 64;  // 256 bytes
+static __device__ __align__(256) uint32_t g_noalloc_queue[kNoAllocHeaderWords + HIVE_NOALLOC_MAX_OPS];
+
+constexpr int kMaxDevices = 64;
+void* g_noalloc_addr[kMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+// Device address of g_noalloc_queue on the current device (dev), looked up once per device.
+int noalloc_queue(int dev, uint32_t** out) {
+    if (dev < 0 || dev >= kMaxDevices) return HIVE_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_queue);
+        if (e != cudaSuccess) return cuda_fail(e);
+        g_noalloc_addr[dev] = p;
+    }
+    *out = (uint32_t*)g_noalloc_addr[dev];
+    return HIVE_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int hive_insert_noalloc(hive_table* h, const uint32_t* keys, const uint32_t* values, uint64_t n, uint8_t* status,
+                        void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n > HIVE_NOALLOC_MAX_OPS) return HIVE_ERR_TOO_LARGE;
+    if (n == 0) return HIVE_OK;
+    if (!keys || !values) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    if (!g.ok) return HIVE_ERR_CUDA;
+    uint32_t* base = nullptr;
+    int rc = noalloc_queue(h->device, &base);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    Defer d{base + kNoAllocHeaderWords, (u64*)base};
+    HIVE_CUDA(cudaMemsetAsync(d.n, 0, sizeof(u64), s));  // the queue count must start at zero
+    HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, n, status, d);
+    HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, d);
     return launch_check();
 }
 

@@ -28,6 +28,7 @@ ERRORS = {
     5: "HIVE_ERR_RETRY_LIMIT",
     6: "HIVE_ERR_CAPACITY",
     7: "HIVE_ERR_NO_DEVICE",
+    8: "HIVE_ERR_TOO_LARGE",
 }
 ST_FAIL, ST_INSERTED, ST_UPDATED, ST_STASHED, ST_ERROR = 0, 1, 2, 3, 255
 OP_INSERT, OP_LOOKUP, OP_DELETE, OP_INCREMENT, OP_NONE = 0, 1, 2, 3, 4
@@ -74,6 +75,7 @@ ABI = [
     ("hive_destroy", _I32, [_P]),
     ("hive_clear", _I32, [_P, _P]),
     ("hive_insert", _I32, [_P, _P, _P, _U64, _P, _P]),
+    ("hive_insert_noalloc", _I32, [_P, _P, _P, _U64, _P, _P]),
     ("hive_find", _I32, [_P, _P, _U64, _P, _P, _P]),
     ("hive_erase", _I32, [_P, _P, _U64, _P, _P]),
     ("hive_apply_ops", _I32, [_P, _P, _P, _P, _U64, _P, _P, _U32, _P]),

@@ -119,6 +119,27 @@ int hive_clear(hive_table* t, void* stream);
 int hive_insert(hive_table* t, const uint32_t* keys, const uint32_t* values, uint64_t n,
                 uint8_t* status, void* stream);
 
+/* hive_insert without any device allocation.  No counterpart in the reference.
+ *
+ * hive_insert keeps its second-pass queue (4 bytes per op) in device memory that it allocates,
+ * and grows with cudaMalloc the first time a batch is larger than any before.  Some callers
+ * cannot allow that: a service that hands all device memory to its own pool up front, a
+ * latency-bound loop where cudaMalloc/cudaFree would stall the device, code under an allocator
+ * that forbids raw device allocations.  This entry point uses instead a fixed queue compiled
+ * into the library (HIVE_NOALLOC_MAX_OPS entries, 4 MiB plus a 256-byte header, resident on every
+ * GPU that loads the library until the process exits) and makes no allocation of any kind.
+ *   - n > HIVE_NOALLOC_MAX_OPS is rejected with HIVE_ERR_TOO_LARGE before any work is queued.
+ *   - The first call on each device looks up the queue's device address (cudaGetSymbolAddress)
+ *     with that device current; make that first call before any stream capture.
+ *   - All calls share the one queue: calls whose work overlaps on the GPU (other streams, other
+ *     threads, other tables) race and must be ordered by the caller.  Each call resets the queue
+ *     count on `stream` before using it; the queue keeps the last call's contents otherwise.
+ * Results and semantics are those of hive_insert. */
+#define HIVE_NOALLOC_MAX_OPS (1u << 20)
+#define HIVE_ERR_TOO_LARGE 8 /* batch larger than HIVE_NOALLOC_MAX_OPS */
+int hive_insert_noalloc(hive_table* t, const uint32_t* keys, const uint32_t* values, uint64_t n,
+                        uint8_t* status, void* stream);
+
 /* Bulk lookup: values[i] = value of keys[i] (0 if absent), found[i] = 0/1.  Either output may be
  * NULL.  Must not overlap on the GPU with a call that modifies the same table.
  * Replaces hive_lookup_kernel (include/hive_kernels.cuh:76-117), which discards the value. */
