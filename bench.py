@@ -62,6 +62,18 @@ def parse_args():
     return ap.parse_args()
 
 
+def launches_per_step(cap, n_ins, n_look):
+    """Kernels of this library launched per step: clear (k_clear_stash); insert (region
+    histogram, scan, scatter, first pass, deferred pass, status scatter when the batch is
+    region-ordered, else the two passes); lookup (histogram, scan, scatter, k_find, output
+    scatter, else k_find).  Region ordering applies when ops >= buckets >= 2^17."""
+    nb = cap // 8
+    reg = lambda n: nb >= (1 << 17) and n >= nb
+    share = n_ins / cap
+    nsub = 1 if share <= 0.25 else 2 if share <= 0.5 else 4 if share <= 0.75 else 8
+    return 1 + (4 + 2 * nsub if reg(n_ins) else 2) + (5 if reg(n_look) else 1)
+
+
 def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -380,7 +392,7 @@ def main():
                 "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seeded uint32 keys/values)",
                 "config": workload_config(args, world), "roofline": roof, "roofline_all": rl,
                 "insert_mops": rl["k_insert"]["mops"], "lookup_mops": rl["k_find"]["mops"],
-                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": 4 * args.steps,
+                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches_per_step(cap, n, n_look) * args.steps,
                 "insert_counters": step_counters, "random_bucket_ceiling": ceiling,
                 "clocks": sampler.summary()}
         print(json.dumps(line), flush=True)

@@ -90,8 +90,20 @@ def build_probe(force: bool = False) -> Path:
     return out
 
 
+def build_serve(force: bool = False) -> Path:
+    out = LIB / "libhive_serve.so"
+    src = CSRC / "hive_serve.cpp"
+    core = build_core(force=False)
+    if force or _stale(out, [src, core, INCLUDE / "hive_c.h", INCLUDE / "hive_serve.h"]):
+        LIB.mkdir(exist_ok=True)
+        _run([_nvcc(), "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+              f"-I{INCLUDE}", str(src), "-o", str(out), f"-L{LIB}", "-lhive_b200", "-Xlinker", "-rpath=$ORIGIN",
+              "-lcudart"])
+    return out
+
+
 def build_all(force: bool = False) -> list[Path]:
-    outs = [build_core(force), build_workload(force), build_probe(force)]
+    outs = [build_core(force), build_workload(force), build_probe(force), build_serve(force)]
     if (CSRC / "hive_compat.cpp").exists():
         outs.append(build_compat(force))
     return outs

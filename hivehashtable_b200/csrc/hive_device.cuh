@@ -11,8 +11,9 @@
 //                                keeps this as bit 31 of a per-bucket freeMask word,
 //                                include/hive_hash_insert.cuh:512-514); 1 bit per bucket keeps
 //                                it L2-resident (1 MiB at 2^23 buckets)
-//   lock_bits  u32[nb_cap / 32]  eviction locks, 1 bit per bucket (the reference uses a u32
-//                                word per bucket, include/hive_hash_table_struct.cuh:101-117)
+//   locks      u32[nb_cap]       eviction locks, one word per bucket as in the reference
+//                                (include/hive_hash_table_struct.cuh:101-117): a word per bucket
+//                                keeps evictors of unrelated buckets off each other's words
 //   full_bits  u32[nb_cap / 32]  bit b set = bucket b was seen full (set by the claim that took
 //                                its last free slot, cleared by deletes).  A hint only: the
 //                                evictor reads it for all 8 victims' alternate buckets at once
@@ -69,7 +70,7 @@ struct Table {
     u64* slots;
     u64* stash;
     uint32_t* stash_bits;
-    uint32_t* lock_bits;
+    uint32_t* locks;
     uint32_t* full_bits;
     u64* counters;
     u64 m_lo;  // fastmod magic for n_lo
@@ -263,16 +264,18 @@ __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gp
 constexpr int kRetryLimit = 64;       // CAS retries of one op on one bucket
 constexpr int kLockSpinLimit = 1 << 16;  // lock attempts before the wait is declared expired
 
-// Bounded test-and-set on the bucket's lock bit with acquire semantics.  Returns false when the
-// wait expired.
+// Bounded test-and-set on the bucket's lock word.  Returns false when the wait expired.
+//
+// The lock only excludes other evictors of the same bucket; every table access made while it is
+// held is itself a gpu-scope CAS or a strong (ld.relaxed.gpu) load, each completed (its result
+// consumed) before the next is issued, and all of them are performed at L2, the point of
+// coherence.  The only fire-and-forget writes are the full-bucket hints and the stash flag, and
+// the stash flag is published before its entry (see insert_locked).  So relaxed lock operations
+// suffice and no fence is paid per eviction.
 __device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
-    uint32_t* w = t.lock_bits + (b >> 5);
-    const uint32_t bit = 1u << (b & 31);
     unsigned ns = 32;
     for (int i = 0; i < kLockSpinLimit; ++i) {
-        uint32_t old;
-        asm volatile("atom.acquire.gpu.global.or.b32 %0, [%1], %2;" : "=r"(old) : "l"(w), "r"(bit) : "memory");
-        if (!(old & bit)) return true;
+        if (atomicCAS(t.locks + b, 0u, 1u) == 0u) return true;
         __nanosleep(ns);
         if (ns < 1024) ns <<= 1;
     }
@@ -280,10 +283,7 @@ __device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
     raise_error(t, kErrLockTimeout);
     return false;
 }
-__device__ __forceinline__ void unlock_bucket(const Table& t, uint32_t b) {
-    asm volatile("red.release.gpu.global.and.b32 [%0], %1;" ::"l"(t.lock_bits + (b >> 5)), "r"(~(1u << (b & 31)))
-                 : "memory");
-}
+__device__ __forceinline__ void unlock_bucket(const Table& t, uint32_t b) { atomicExch(t.locks + b, 0u); }
 
 // ---------------------------------------------------------------------------------------------
 // Lookup: H0, H1, then the canonical stash gated by its flag
@@ -525,8 +525,7 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         if (ev == kEvRetry) continue;
         // Stage D: the canonical bucket's stash.  Its flag is raised before the entry is
         // written, so a reader that finds the entry also finds the flag set.
-        atomicOr(t.stash_bits + (b0 >> 5), 1u << (b0 & 31));
-        fence_acq_rel();
+        if (!(atomicOr(t.stash_bits + (b0 >> 5), 1u << (b0 & 31)) & (1u << (b0 & 31)))) fence_acq_rel();
         for (int q = 0; q < kRetryLimit; ++q) {
             Bucket S;
             load_bucket(Sp, S);
@@ -576,16 +575,21 @@ __device__ __forceinline__ uint8_t claim_or_update(const Table& t, uint32_t b, u
 // by the host (which knows the flags) so the kernel carries only the code it needs.
 enum Mode { kModeRuntime = 0, kModeMono = 1, kModeHoles = 2 };
 
-// Lock-free stages A and B.  Returns the op's final status, or 0 when H0 and H1 are both full
-// and the locked path (stages C/D) is needed.
-template <int P, int kMode = kModeRuntime>
+// Lock-free stages A and B.  Returns the op's final status, or 0 when the op must go on: to the
+// locked path (stages C/D) when H0 and H1 are both full, or -- with kPrimaryOnly, the first pass
+// of a two-pass insert -- as soon as H0 is full.  Claiming only in H0 in the first pass and
+// leaving every claim in H1 to the second pass fills the table primary-first: no key's overflow
+// takes an H0 slot that one of that bucket's own keys would claim later in the same batch.  This
+// keeps the final placement independent of the order the batch is processed in (including the
+// region order of large batches) and leaves more keys in H0, where lookups find them first.
+template <int P, int kMode = kModeRuntime, bool kPrimaryOnly = false>
 __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
     u64* B0p = t.slots + (size_t)b0 * kSlots;
     u64* B1p = t.slots + (size_t)b1 * kSlots;
     const bool holes = kMode == kModeHoles || (kMode == kModeRuntime && (t.flags & kFlagHoles));
     if (!holes) {
         uint8_t st = claim_or_update(t, b0, k, kv);
-        if (st || b1 == b0) return st;
+        if (st || b1 == b0 || kPrimaryOnly) return st;
         return claim_or_update(t, b1, k, kv);
     }
     // With holes a key may sit in H1 or the stash while H0 has room: scan all three first.
@@ -616,7 +620,7 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
         uint32_t e = empty_mask(B0);
         u64* Cp = B0p;
         uint32_t cb = b0;
-        if (!e && b1 != b0) {
+        if (!e && b1 != b0 && !kPrimaryOnly) {
             e = empty_mask(B1);
             Cp = B1p;
             cb = b1;
@@ -649,9 +653,25 @@ __device__ __forceinline__ uint8_t insert_one(const Table& t, uint32_t k, uint32
     const u64 kv = pack(k, v);
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
     const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
-    uint8_t st = insert_lockfree<P, kMode>(t, k, kv, b0, b1);
+    uint8_t st = insert_lockfree<P, kMode, kDefer>(t, k, kv, b0, b1);
     if (st) return st;
     if (kDefer) return kStDefer;
+    return insert_locked_path<P>(t, k, kv, b0, b1);
+}
+
+// A deferred op in the second pass.  Without holes its H0 was full in the first pass and stays
+// full, so it claims (or updates) in H1 without a lock and takes the locked path only if H1 is
+// full too; with holes the whole protocol runs again (a slot may have freed up since).
+template <int P>
+__device__ __forceinline__ uint8_t insert_deferred_one(const Table& t, uint32_t k, uint32_t v) {
+    if (t.flags & kFlagHoles) return insert_one<P>(t, k, v);
+    const u64 kv = pack(k, v);
+    const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
+    const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
+    if (b1 != b0) {
+        const uint8_t st = claim_or_update(t, b1, k, kv);
+        if (st) return st;
+    }
     return insert_locked_path<P>(t, k, kv, b0, b1);
 }
 

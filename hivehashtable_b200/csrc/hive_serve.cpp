@@ -1,0 +1,293 @@
+// hive_serve.cpp -- an open-loop request loop with continuous batching over one Hive table.
+//
+// The reference has no serving path (its "YCSB" driver is one closed-loop bulk launch,
+// src/hashTableBenchmark.cc:434-570).  This loop admits requests by arrival time and keeps the
+// GPU fed with batches:
+//
+//   admit      every request whose arrival time has passed joins the pending queue
+//   coalesce   a batch takes up to max_batch pending requests in arrival order and groups them
+//              by key: a group whose first request is a lookup needs the key's value before the
+//              batch (one device lookup); a group with writes needs one device upsert of its last
+//              written value.  Lookups after a write in the same batch are answered from that
+//              write, so every result equals the one a one-at-a-time replay in arrival order gives
+//   launch     pinned-host -> device copies on the slot's copy stream; the lookups, then the
+//              upserts, on the single compute stream (batches therefore reach the table in
+//              arrival order); the results back on the copy stream
+//   pipeline   up to `depth` batches are in flight: while the GPU works on one, the next batch is
+//              formed, copied and queued.  depth = 1 is the plain loop: one synchronous batch at
+//              a time
+//   growth     before a batch that could push the load factor past max_load, the loop drains,
+//              checks free device memory for the doubled table (cudaMemGetInfo) and grows it
+//              with hive_resize; when memory does not allow it, the batch's new keys are refused
+//              (status 0) and existing keys still update
+//
+// Completion time of a request = when its batch's results are on the host and answered.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <unordered_map>
+#include <vector>
+
+#include "hive_serve.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Slot {
+    cudaStream_t copy = nullptr;
+    cudaEvent_t staged = nullptr, done = nullptr;
+    // pinned host staging
+    uint32_t *h_fkeys = nullptr, *h_ukeys = nullptr, *h_uvals = nullptr, *h_fvals = nullptr;
+    uint8_t *h_types = nullptr, *h_ftypes = nullptr, *h_found = nullptr, *h_ust = nullptr;
+    // device
+    uint32_t *d_fkeys = nullptr, *d_ukeys = nullptr, *d_uvals = nullptr, *d_fvals = nullptr;
+    uint8_t *d_ftypes = nullptr, *d_utypes = nullptr, *d_found = nullptr, *d_ust = nullptr;
+    // the batch
+    std::vector<uint64_t> req;        // request indices, arrival order
+    std::vector<int32_t> group;       // group of each request
+    std::vector<int32_t> find_of;     // group -> position in the lookup list or -1
+    std::vector<int32_t> upsert_of;   // group -> position in the upsert list or -1
+    uint32_t nf = 0, nu = 0;
+    bool busy = false;
+};
+
+int alloc_slot(Slot& s, uint32_t cap) {
+    if (cudaStreamCreateWithFlags(&s.copy, cudaStreamNonBlocking) != cudaSuccess) return HIVE_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&s.staged, cudaEventDisableTiming) != cudaSuccess) return HIVE_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) return HIVE_ERR_CUDA;
+    const size_t w = (size_t)cap * 4, b = (size_t)cap;
+    if (cudaMallocHost(&s.h_fkeys, w) || cudaMallocHost(&s.h_ukeys, w) || cudaMallocHost(&s.h_uvals, w) ||
+        cudaMallocHost(&s.h_fvals, w) || cudaMallocHost(&s.h_types, b) || cudaMallocHost(&s.h_ftypes, b) ||
+        cudaMallocHost(&s.h_found, b) || cudaMallocHost(&s.h_ust, b))
+        return HIVE_ERR_OOM;
+    if (cudaMalloc(&s.d_fkeys, w) || cudaMalloc(&s.d_ukeys, w) || cudaMalloc(&s.d_uvals, w) ||
+        cudaMalloc(&s.d_fvals, w) || cudaMalloc(&s.d_ftypes, b) || cudaMalloc(&s.d_utypes, b) ||
+        cudaMalloc(&s.d_found, b) || cudaMalloc(&s.d_ust, b))
+        return HIVE_ERR_OOM;
+    std::memset(s.h_ftypes, HIVE_OP_LOOKUP, b);
+    std::memset(s.h_types, HIVE_OP_INSERT, b);
+    if (cudaMemcpy(s.d_ftypes, s.h_ftypes, b, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(s.d_utypes, s.h_types, b, cudaMemcpyHostToDevice))
+        return HIVE_ERR_CUDA;
+    return HIVE_OK;
+}
+
+void free_slot(Slot& s) {
+    cudaFreeHost(s.h_fkeys); cudaFreeHost(s.h_ukeys); cudaFreeHost(s.h_uvals); cudaFreeHost(s.h_fvals);
+    cudaFreeHost(s.h_types); cudaFreeHost(s.h_ftypes); cudaFreeHost(s.h_found); cudaFreeHost(s.h_ust);
+    cudaFree(s.d_fkeys); cudaFree(s.d_ukeys); cudaFree(s.d_uvals); cudaFree(s.d_fvals);
+    cudaFree(s.d_ftypes); cudaFree(s.d_utypes); cudaFree(s.d_found); cudaFree(s.d_ust);
+    if (s.staged) cudaEventDestroy(s.staged);
+    if (s.done) cudaEventDestroy(s.done);
+    if (s.copy) cudaStreamDestroy(s.copy);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hive_serve_run(
+    hive_table* t, const hive_serve_config* cfg, const uint8_t* types, const uint32_t* keys, const uint32_t* vals,
+    const double* arrival_s, uint64_t n, uint32_t* out_vals, uint8_t* out_status, double* done_s,
+    hive_serve_stats* stats) {
+    if (!t || !cfg || !types || !keys || !vals || !arrival_s || !out_vals || !out_status || !done_s)
+        return HIVE_ERR_INVALID_ARG;
+    if (cfg->depth < 1 || cfg->depth > 64 || cfg->max_batch < 1) return HIVE_ERR_INVALID_ARG;
+    hive_serve_stats st{};
+    const uint32_t cap = cfg->max_batch;
+    std::vector<Slot> slots(cfg->depth);
+    int rc = HIVE_OK;
+    cudaStream_t compute = nullptr;
+    if (cudaStreamCreateWithFlags(&compute, cudaStreamNonBlocking) != cudaSuccess) return HIVE_ERR_CUDA;
+    for (auto& s : slots)
+        if ((rc = alloc_slot(s, cap))) break;
+    hive_info info{};
+    uint64_t live = cfg->live_keys;
+
+    std::unordered_map<uint32_t, int32_t> gid;
+    gid.reserve(cap * 2);
+    std::deque<uint64_t> pending;   // request indices waiting, arrival order
+    std::vector<uint32_t> g_lastw;  // group -> index (into slot.req) of its last write, or -1
+    uint64_t next = 0, finished = 0;
+    size_t head = 0;                // ring position of the oldest in-flight slot
+    size_t in_flight = 0;
+    const auto t0 = Clock::now();
+    auto now_s = [&] { return std::chrono::duration<double>(Clock::now() - t0).count(); };
+
+    auto finish = [&](Slot& s) {
+        // answers of the batch, in request order
+        std::vector<int32_t> lastw(s.find_of.size(), -1);
+        for (size_t j = 0; j < s.req.size(); ++j) {
+            const uint64_t r = s.req[j];
+            const int32_t g = s.group[j];
+            if (types[r] == HIVE_OP_LOOKUP) {
+                if (lastw[g] >= 0) {
+                    out_vals[r] = vals[s.req[lastw[g]]];
+                    out_status[r] = 1;
+                } else {
+                    const int32_t f = s.find_of[g];
+                    out_status[r] = s.h_found[f];
+                    out_vals[r] = s.h_found[f] ? s.h_fvals[f] : 0u;
+                }
+            } else {
+                lastw[g] = (int32_t)j;
+                const int32_t u = s.upsert_of[g];
+                const uint8_t us = u >= 0 ? s.h_ust[u] : 0;
+                out_status[r] = (us != HIVE_ST_FAIL && us != HIVE_ST_ERROR) ? 1 : 0;
+                out_vals[r] = 0;
+            }
+        }
+        const double td = now_s();
+        for (uint64_t r : s.req) done_s[r] = td;
+        finished += s.req.size();
+        s.busy = false;
+    };
+
+    auto drain = [&] {
+        while (in_flight) {
+            Slot& s = slots[head];
+            if (cudaEventSynchronize(s.done) != cudaSuccess) return HIVE_ERR_CUDA;
+            finish(s);
+            head = (head + 1) % slots.size();
+            --in_flight;
+        }
+        return HIVE_OK;
+    };
+
+    size_t tail = 0;  // next slot to fill
+    while (!rc && finished < n) {
+        // admit arrivals
+        const double tn = now_s();
+        while (next < n && arrival_s[next] <= tn) pending.push_back(next++);
+        // retire completed batches in order
+        while (in_flight) {
+            Slot& s = slots[head];
+            const cudaError_t q = cudaEventQuery(s.done);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) { rc = HIVE_ERR_CUDA; break; }
+            finish(s);
+            head = (head + 1) % slots.size();
+            --in_flight;
+        }
+        if (rc) break;
+        if (pending.empty() || in_flight == slots.size()) {
+            if (pending.empty() && next < n && in_flight == 0) {
+                // idle until the next arrival
+                while (now_s() < arrival_s[next]) {
+                }
+            }
+            continue;
+        }
+        // form a batch
+        Slot& s = slots[tail];
+        const size_t take = std::min<size_t>(pending.size(), cap);
+        s.req.assign(pending.begin(), pending.begin() + take);
+        pending.erase(pending.begin(), pending.begin() + take);
+        gid.clear();
+        s.group.resize(take);
+        s.find_of.clear();
+        s.upsert_of.clear();
+        g_lastw.clear();
+        uint64_t new_writes = 0;
+        for (size_t j = 0; j < take; ++j) {
+            const uint64_t r = s.req[j];
+            auto it = gid.find(keys[r]);
+            int32_t g;
+            if (it == gid.end()) {
+                g = (int32_t)s.find_of.size();
+                gid.emplace(keys[r], g);
+                s.find_of.push_back(types[r] == HIVE_OP_LOOKUP ? -2 : -1);  // -2: needs a lookup
+                s.upsert_of.push_back(-1);
+                g_lastw.push_back(0xFFFFFFFFu);
+            } else {
+                g = it->second;
+            }
+            s.group[j] = g;
+            if (types[r] != HIVE_OP_LOOKUP) {
+                if (g_lastw[g] == 0xFFFFFFFFu) ++new_writes;
+                g_lastw[g] = (uint32_t)j;
+            }
+        }
+        s.nf = s.nu = 0;
+        for (size_t g = 0; g < s.find_of.size(); ++g) {
+            if (s.find_of[g] == -2) {
+                s.h_fkeys[s.nf] = 0;
+                s.find_of[g] = (int32_t)s.nf++;
+            } else {
+                s.find_of[g] = -1;
+            }
+            if (g_lastw[g] != 0xFFFFFFFFu) {
+                const uint64_t r = s.req[g_lastw[g]];
+                s.h_ukeys[s.nu] = keys[r];
+                s.h_uvals[s.nu] = vals[r];
+                s.upsert_of[g] = (int32_t)s.nu++;
+            }
+        }
+        for (const auto& kv : gid)
+            if (s.find_of[kv.second] >= 0) s.h_fkeys[s.find_of[kv.second]] = kv.first;
+        // growth: keep the load factor under max_load counting every write as a possible new key
+        if (cfg->max_load > 0.0 && new_writes) {
+            hive_get_info(t, &info);
+            const double cap_slots = (double)info.capacity_slots;
+            if ((double)(live + new_writes) > cfg->max_load * cap_slots) {
+                if ((rc = drain())) break;
+                uint64_t sz = 0;
+                if ((rc = hive_size(t, &sz, compute))) break;
+                live = sz;
+                if ((double)(live + new_writes) > cfg->max_load * cap_slots) {
+                    size_t fr = 0, tot = 0;
+                    cudaMemGetInfo(&fr, &tot);
+                    const double need = cap_slots / 8.0 * 140.0 * 1.1;  // slots+stash+metadata of the doubled part
+                    if ((double)fr > need && hive_resize(t, info.capacity_slots * 2, compute) == HIVE_OK) {
+                        ++st.resizes;
+                    } else {
+                        st.refused += new_writes;  // the batch still runs; inserts that find no room fail
+                    }
+                }
+            }
+        }
+        live += new_writes;
+        // launch
+        if (s.nf && cudaMemcpyAsync(s.d_fkeys, s.h_fkeys, (size_t)s.nf * 4, cudaMemcpyHostToDevice, s.copy)) rc = HIVE_ERR_CUDA;
+        if (s.nu && (cudaMemcpyAsync(s.d_ukeys, s.h_ukeys, (size_t)s.nu * 4, cudaMemcpyHostToDevice, s.copy) ||
+                     cudaMemcpyAsync(s.d_uvals, s.h_uvals, (size_t)s.nu * 4, cudaMemcpyHostToDevice, s.copy)))
+            rc = HIVE_ERR_CUDA;
+        if (rc) break;
+        cudaEventRecord(s.staged, s.copy);
+        cudaStreamWaitEvent(compute, s.staged, 0);
+        if (s.nf && (rc = hive_apply_ops(t, s.d_ftypes, s.d_fkeys, nullptr, s.nf, s.d_found, s.d_fvals,
+                                         HIVE_HINT_NO_DELETES, compute)))
+            break;
+        if (s.nu && (rc = hive_apply_ops(t, s.d_utypes, s.d_ukeys, s.d_uvals, s.nu, s.d_ust, nullptr,
+                                         HIVE_HINT_NO_DELETES, compute)))
+            break;
+        cudaEventRecord(s.done, compute);
+        cudaStreamWaitEvent(s.copy, s.done, 0);
+        if (s.nf && (cudaMemcpyAsync(s.h_found, s.d_found, s.nf, cudaMemcpyDeviceToHost, s.copy) ||
+                     cudaMemcpyAsync(s.h_fvals, s.d_fvals, (size_t)s.nf * 4, cudaMemcpyDeviceToHost, s.copy)))
+            rc = HIVE_ERR_CUDA;
+        if (s.nu && cudaMemcpyAsync(s.h_ust, s.d_ust, s.nu, cudaMemcpyDeviceToHost, s.copy)) rc = HIVE_ERR_CUDA;
+        cudaEventRecord(s.done, s.copy);
+        st.batches++;
+        st.device_lookups += s.nf;
+        st.device_upserts += s.nu;
+        s.busy = true;
+        tail = (tail + 1) % slots.size();
+        ++in_flight;
+    }
+    if (!rc) rc = drain();
+    if (!rc) rc = hive_check(t, compute);
+    st.wall_s = now_s();
+    if (stats) *stats = st;
+    cudaStreamSynchronize(compute);
+    for (auto& s : slots) free_slot(s);
+    cudaStreamDestroy(compute);
+    return rc;
+}
+
+}  // extern "C"

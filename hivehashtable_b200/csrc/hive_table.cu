@@ -14,10 +14,13 @@
 #include <mutex>
 #include <new>
 
+#include <cooperative_groups.h>
+
 #include "hive_c.h"
 #include "hive_device.cuh"
 
 using hive::u64;
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -69,6 +72,8 @@ struct hive_table {
     u64* scratch = nullptr;  // device words: [0] size/dump count, [1] deferred-op count
     uint32_t* defer_q = nullptr;  // deferred-op queue (one index per op of the largest batch)
     uint64_t defer_cap = 0;
+    void* rbuf = nullptr;         // region-ordering buffers (13 bytes per op of the largest batch)
+    uint64_t rcap = 0;
     int num_sms = 148;
 };
 
@@ -96,7 +101,7 @@ Carve carve(uint64_t nb_cap) {
     c.stash = align256(c.slots + (size_t)nb_cap * 64);
     c.sbits = align256(c.stash + (size_t)nb_cap * 64);
     c.lbits = align256(c.sbits + words * 4);
-    c.fbits = align256(c.lbits + words * 4);
+    c.fbits = align256(c.lbits + (size_t)nb_cap * 4);
     c.ctr = align256(c.fbits + words * 4);
     c.scratch = align256(c.ctr + HIVE_NUM_COUNTERS * 8);
     c.total = align256(c.scratch + 16);
@@ -112,7 +117,7 @@ void bind_arrays(hive_table* h, void* block, uint64_t nb_cap) {
     h->t.slots = (u64*)(base + c.slots);
     h->t.stash = (u64*)(base + c.stash);
     h->t.stash_bits = (uint32_t*)(base + c.sbits);
-    h->t.lock_bits = (uint32_t*)(base + c.lbits);
+    h->t.locks = (uint32_t*)(base + c.lbits);
     h->t.full_bits = (uint32_t*)(base + c.fbits);
     h->t.counters = (u64*)(base + c.ctr);
     h->scratch = (u64*)(base + c.scratch);
@@ -128,6 +133,14 @@ struct Defer {
     uint32_t* q;
     u64* n;
 };
+
+// The second pass visits queue position defer_slot(j, cnt) at step j: a bijection of [0, cnt)
+// (multiplication by a prime larger than any queue), so the deferred ops -- appended in the
+// first pass's order, which for a region-ordered batch is bucket order -- are finished in an
+// order unrelated to their buckets.  Finished in bucket order, the last buckets' overflow would
+// meet alternate buckets already filled by all earlier overflow and exhaust their stashes.
+// (j < cnt < 2^32, so j * (p mod cnt) < 2^64; gcd(p mod cnt, cnt) = gcd(p, cnt) = 1.)
+__device__ __forceinline__ u64 defer_slot(u64 j, u64 cnt) { return (j * (4294967311ull % cnt)) % cnt; }
 
 // Appends index i for every lane whose st is kStDefer, one atomic per warp.  Every lane of the
 // warp must call it.
@@ -157,15 +170,130 @@ __global__ void __launch_bounds__(kBlock, (kDefer && kMode == hive::kModeMono) ?
 
 // Second pass: the deferred inserts, grid-stride over the queue.
 template <int P>
-__global__ void __launch_bounds__(kBlock) k_insert_deferred(hive::Table t, const uint32_t* __restrict__ keys,
+__global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, const uint32_t* __restrict__ keys,
                                                             const uint32_t* __restrict__ vals,
                                                             uint8_t* __restrict__ status, Defer d) {
     const u64 cnt = *d.n;
     for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
-        const uint32_t i = d.q[j];
-        const uint8_t st = hive::insert_one<P>(t, keys[i], vals[i]);
+        const uint32_t i = d.q[defer_slot(j, cnt)];
+        const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals[i]);
         if (status) status[i] = st;
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Region ordering for large bulk batches.  A batch with about one op per bucket or more touches
+// every bucket several times; processed in arrival order each touch is a random HBM access.
+// Reordered by region (2^rshift consecutive buckets, >= 2 MiB of table), the blocks in flight at
+// any moment cover a few regions, so after a region's first touches its buckets are served by
+// L2 and each table line crosses HBM about once per batch.  The reorder is a counting sort by
+// region over (key, value, index): one histogram pass, a scan of the region counts, one scatter
+// pass (sequential traffic), and at the end one scatter of the per-op outputs back to the
+// caller's order.
+// ---------------------------------------------------------------------------------------------
+constexpr int kMinRegionShift = 15;       // >= 32768 buckets = 2 MiB of slots per region
+constexpr int kMaxRegions = 1024;
+constexpr int kRegionTile = kBlock * 8;   // ops per block in the histogram and scatter passes
+
+// Sort bin of op i: its sub-batch (a contiguous share of the caller's order, i * nsub / n) major,
+// its region minor.  Sub-batches let a batch that adds much of the table's capacity fill it in
+// nsub rounds -- each a first pass and a deferred pass -- as an online insert order would, rather
+// than handling all of its overflow at the end when every bucket holds its final primaries.
+__device__ __forceinline__ uint32_t region_bin(const hive::Table& t, uint32_t h0, uint64_t i, uint64_t n, int nreg,
+                                               int rshift, int nsub) {
+    const uint32_t sub = nsub > 1 ? (uint32_t)((i * (uint64_t)nsub) / n) : 0u;
+    return sub * (uint32_t)nreg + (hive::bucket_addr(t, h0) >> rshift);
+}
+
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_region_hist(hive::Table t, const uint32_t* __restrict__ keys, uint64_t n,
+                                                        int nreg, int rshift, int nsub, uint32_t* __restrict__ counts) {
+    const int nbin = nreg * nsub;
+    __shared__ uint32_t hist[kMaxRegions];
+    for (int r = threadIdx.x; r < nbin; r += kBlock) hist[r] = 0;
+    __syncthreads();
+    const uint64_t base = (uint64_t)blockIdx.x * kRegionTile;
+    for (int q = threadIdx.x; q < kRegionTile; q += kBlock) {
+        const uint64_t i = base + q;
+        if (i < n) atomicAdd(&hist[region_bin(t, hive::Policy<P>::h0(__ldg(keys + i)), i, n, nreg, rshift, nsub)], 1u);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nbin; r += kBlock)
+        if (hist[r]) atomicAdd(counts + r, hist[r]);
+}
+
+// Exclusive scan of the region counts into cursors (one block; nreg <= kMaxRegions).
+__global__ void __launch_bounds__(kMaxRegions) k_region_scan(const uint32_t* __restrict__ counts, int nreg,
+                                                             uint32_t* __restrict__ cursors) {
+    __shared__ uint32_t s[kMaxRegions];
+    const int r = threadIdx.x;
+    const uint32_t c = r < nreg ? counts[r] : 0u;
+    s[r] = c;
+    __syncthreads();
+    for (int o = 1; o < kMaxRegions; o <<= 1) {
+        const uint32_t y = r >= o ? s[r - o] : 0u;
+        __syncthreads();
+        s[r] += y;
+        __syncthreads();
+    }
+    if (r < nreg) cursors[r] = s[r] - c;
+}
+
+// Scatter (key, value, index) of each op to its region's next free positions.  vals may be null.
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_region_scatter(hive::Table t, const uint32_t* __restrict__ keys,
+                                                           const uint32_t* __restrict__ vals, uint64_t n, int nreg,
+                                                           int rshift, int nsub, uint32_t* __restrict__ cursors,
+                                                           uint32_t* __restrict__ rkeys,
+                                                           uint32_t* __restrict__ rvals, uint32_t* __restrict__ ridx) {
+    __shared__ uint32_t hist[kMaxRegions];
+    __shared__ uint32_t start[kMaxRegions];
+    constexpr int kPer = kRegionTile / kBlock;
+    const int nbin = nreg * nsub;
+    for (int r = threadIdx.x; r < nbin; r += kBlock) hist[r] = 0;
+    __syncthreads();
+    const uint64_t base = (uint64_t)blockIdx.x * kRegionTile;
+    uint32_t k[kPer], reg[kPer], rank[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const uint64_t i = base + (uint64_t)q * kBlock + threadIdx.x;
+        reg[q] = 0xFFFFFFFFu;
+        if (i < n) {
+            k[q] = __ldcs(keys + i);
+            reg[q] = region_bin(t, hive::Policy<P>::h0(k[q]), i, n, nreg, rshift, nsub);
+            rank[q] = atomicAdd(&hist[reg[q]], 1u);
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nbin; r += kBlock)
+        if (hist[r]) start[r] = atomicAdd(cursors + r, hist[r]);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        if (reg[q] == 0xFFFFFFFFu) continue;
+        const uint64_t i = base + (uint64_t)q * kBlock + threadIdx.x;
+        const uint32_t pos = start[reg[q]] + rank[q];
+        rkeys[pos] = k[q];
+        if (rvals) rvals[pos] = __ldcs(vals + i);
+        ridx[pos] = (uint32_t)i;
+    }
+}
+
+// Outputs back to the caller's order.
+__global__ void __launch_bounds__(kBlock) k_unpermute_u8(const uint32_t* __restrict__ ridx,
+                                                         const uint8_t* __restrict__ src, uint64_t n,
+                                                         uint8_t* __restrict__ dst) {
+    const uint64_t j = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (j < n) dst[__ldcs(ridx + j)] = __ldcs(src + j);
+}
+__global__ void __launch_bounds__(kBlock) k_unpermute_find(const uint32_t* __restrict__ ridx,
+                                                           const uint32_t* __restrict__ sv, const uint8_t* __restrict__ sf,
+                                                           uint64_t n, uint32_t* __restrict__ dv, uint8_t* __restrict__ df) {
+    const uint64_t j = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t i = __ldcs(ridx + j);
+    if (dv) dv[i] = __ldcs(sv + j);
+    if (df) df[i] = __ldcs(sf + j);
 }
 
 template <int P>
@@ -234,16 +362,58 @@ __global__ void __launch_bounds__(kBlock) k_apply(hive::Table t, const uint8_t* 
 
 // Second pass of k_apply: the deferred inserts (their out value is 0).
 template <int P>
-__global__ void __launch_bounds__(kBlock) k_apply_deferred(hive::Table t, const uint32_t* __restrict__ keys,
+__global__ void __launch_bounds__(kBlock, 4) k_apply_deferred(hive::Table t, const uint32_t* __restrict__ keys,
                                                            const uint32_t* __restrict__ vals,
                                                            uint8_t* __restrict__ status, uint32_t* __restrict__ outv,
                                                            Defer d) {
     const u64 cnt = *d.n;
     for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
-        const uint32_t i = d.q[j];
-        const uint8_t st = hive::insert_one<P>(t, keys[i], vals ? vals[i] : 0u);
+        const uint32_t i = d.q[defer_slot(j, cnt)];
+        const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals ? vals[i] : 0u);
         if (status) status[i] = st;
         if (outv) outv[i] = 0u;
+    }
+}
+
+// A sequence of mixed batches in one cooperative launch.  Per batch: a first pass over its ops
+// (warp-uniform grid-stride, so every lane of a warp takes part in each deferral append), a grid
+// barrier, the deferred inserts, a grid barrier.  Two queue counts alternate between batches:
+// batch b appends to count[b & 1], and its deferred pass zeroes count[(b + 1) & 1], which no one
+// uses until the next barrier.  Every block reaches every barrier (no early exit), and the
+// cooperative launch guarantees all blocks are resident, so each barrier completes.
+template <int P, int kMode>
+__global__ void k_apply_batches(hive::Table t, const uint8_t* __restrict__ types, const uint32_t* __restrict__ keys,
+                                const uint32_t* __restrict__ vals, const u64* __restrict__ offsets, uint32_t nbatch,
+                                uint8_t* __restrict__ status, uint32_t* __restrict__ outv, uint32_t* q, u64* qn) {
+    cg::grid_group grid = cg::this_grid();
+    const u64 tid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    const unsigned lane = threadIdx.x & 31;
+    for (uint32_t b = 0; b < nbatch; ++b) {
+        const u64 lo = offsets[b], hi = offsets[b + 1];
+        const Defer d{q, qn + (b & 1)};
+        for (u64 base = lo + (tid - lane); base < hi; base += stride) {
+            const u64 i = base + lane;
+            const bool active = i < hi;
+            uint32_t o = 0;
+            uint8_t st = 0;
+            if (active) st = apply_one<P, true, kMode>(t, types[i], keys[i], vals ? vals[i] : 0u, &o);
+            defer_push(d, st == hive::kStDefer, i);
+            if (active && st != hive::kStDefer) {
+                if (status) status[i] = st;
+                if (outv) outv[i] = o;
+            }
+        }
+        grid.sync();
+        const u64 cnt = *d.n;
+        if (tid == 0) qn[(b + 1) & 1] = 0;
+        for (u64 j = tid; j < cnt; j += stride) {
+            const uint32_t i = q[defer_slot(j, cnt)];
+            const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals ? vals[i] : 0u);
+            if (status) status[i] = st;
+            if (outv) outv[i] = 0u;
+        }
+        grid.sync();
     }
 }
 
@@ -270,13 +440,13 @@ __global__ void __launch_bounds__(kBlock) k_apply_ref(hive::Table t, const ulong
 }
 
 template <int P>
-__global__ void __launch_bounds__(kBlock) k_apply_ref_deferred(hive::Table t, const ulonglong2* __restrict__ ops,
+__global__ void __launch_bounds__(kBlock, 4) k_apply_ref_deferred(hive::Table t, const ulonglong2* __restrict__ ops,
                                                                unsigned long long* __restrict__ results, Defer d) {
     const u64 cnt = *d.n;
     for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
-        const uint32_t i = d.q[j];
+        const uint32_t i = d.q[defer_slot(j, cnt)];
         const uint32_t k = (uint32_t)ops[i].y;
-        const uint8_t st = hive::insert_one<P>(t, k, k + 1u);
+        const uint8_t st = hive::insert_deferred_one<P>(t, k, k + 1u);
         if (results) results[i] = ref_result(st);
     }
 }
@@ -522,7 +692,7 @@ int reset(hive_table* h, cudaStream_t s) {
     int rc = launch_check();
     if (rc) return rc;
     HIVE_CUDA(cudaMemsetAsync(h->t.stash_bits, 0, (size_t)words * 4, s));
-    HIVE_CUDA(cudaMemsetAsync(h->t.lock_bits, 0, (size_t)words * 4, s));
+    HIVE_CUDA(cudaMemsetAsync(h->t.locks, 0, (size_t)nb * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.full_bits, 0, (size_t)words * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.counters, 0, HIVE_NUM_COUNTERS * 8, s));
     return HIVE_OK;
@@ -551,6 +721,79 @@ int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d) {
 
 unsigned second_pass_grid(const hive_table* h, uint64_t n) {
     return (unsigned)std::min<uint64_t>(grid_for(n), (uint64_t)h->num_sms * 4);
+}
+
+// Region ordering pays off when the batch touches each bucket about once or more and the table
+// is well beyond what stays in L2 anyway.
+constexpr uint64_t kRegionMinBuckets = 1ull << 17;  // 8 MiB of slots
+
+struct Regions {
+    int rshift = 0, nreg = 0, nsub = 1;
+    uint32_t *rkeys = nullptr, *rvals = nullptr, *ridx = nullptr, *counts = nullptr, *cursors = nullptr;
+    uint8_t* rst = nullptr;
+};
+
+bool use_regions(const hive_table* h, uint64_t n) {
+    const uint64_t nb = num_buckets(h);
+    return nb >= kRegionMinBuckets && n >= nb && n <= 0xFFFFFFFFull;
+}
+
+// Geometry and buffers of the region ordering for a batch of n ops; the buffers grow
+// (synchronously) to the largest batch seen.
+int prepare_regions(hive_table* h, uint64_t n, int nsub, cudaStream_t s, Regions* r) {
+    const uint64_t nb = num_buckets(h);
+    int sh = kMinRegionShift;
+    while (((nb + (1ull << sh) - 1) >> sh) * (uint64_t)nsub > (uint64_t)kMaxRegions) ++sh;
+    r->nsub = nsub;
+    r->rshift = sh;
+    r->nreg = (int)((nb + (1ull << sh) - 1) >> sh);
+    if (n > h->rcap) {
+        HIVE_CUDA(cudaDeviceSynchronize());
+        if (h->rbuf) cudaFree(h->rbuf);
+        h->rbuf = nullptr;
+        h->rcap = 0;
+        const size_t bytes = align256((size_t)n * 4) * 3 + align256((size_t)n) + 2 * kMaxRegions * 4;
+        cudaError_t e = cudaMalloc(&h->rbuf, bytes);
+        if (e != cudaSuccess) return cuda_fail(e);
+        h->rcap = n;
+    }
+    char* p = (char*)h->rbuf;
+    const size_t w = align256((size_t)h->rcap * 4);
+    r->rkeys = (uint32_t*)p;
+    r->rvals = (uint32_t*)(p + w);
+    r->ridx = (uint32_t*)(p + 2 * w);
+    r->rst = (uint8_t*)(p + 3 * w);
+    r->counts = (uint32_t*)(p + 3 * w + align256((size_t)h->rcap));
+    r->cursors = r->counts + kMaxRegions;
+    HIVE_CUDA(cudaMemsetAsync(r->counts, 0, (size_t)r->nreg * r->nsub * 4, s));
+    return HIVE_OK;
+}
+
+// Sub-batches for a region-ordered insert of n ops: more when the batch adds a larger share of
+// the table's capacity (see region_bin).
+int insert_subbatches(const hive_table* h, uint64_t n) {
+    const double share = (double)n / (double)(num_buckets(h) * hive::kSlots);
+    return share <= 0.25 ? 1 : share <= 0.5 ? 2 : share <= 0.75 ? 4 : 8;
+}
+
+// Counting sort of (key[, value], index) by region into r's buffers.
+int region_sort(hive_table* h, const uint32_t* keys, const uint32_t* vals, uint64_t n, const Regions& r,
+                cudaStream_t s) {
+    const unsigned g = (unsigned)((n + kRegionTile - 1) / kRegionTile);
+    if (h->policy == HIVE_POLICY_MURMURCITYHASH)
+        k_region_hist<1><<<g, kBlock, 0, s>>>(h->t, keys, n, r.nreg, r.rshift, r.nsub, r.counts);
+    else
+        k_region_hist<0><<<g, kBlock, 0, s>>>(h->t, keys, n, r.nreg, r.rshift, r.nsub, r.counts);
+    k_region_scan<<<1, kMaxRegions, 0, s>>>(r.counts, r.nreg * r.nsub, r.cursors);
+    uint32_t* rv = vals ? r.rvals : nullptr;
+    if (h->policy == HIVE_POLICY_MURMURCITYHASH)
+        k_region_scatter<1><<<g, kBlock, 0, s>>>(h->t, keys, vals, n, r.nreg, r.rshift, r.nsub, r.cursors, r.rkeys, rv,
+                                                 r.ridx);
+    else
+        k_region_scatter<0><<<g, kBlock, 0, s>>>(h->t, keys, vals, n, r.nreg, r.rshift, r.nsub, r.cursors, r.rkeys, rv,
+                                                 r.ridx);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? HIVE_OK : cuda_fail(e);
 }
 
 int grow_capacity(hive_table* h, uint64_t need_buckets, cudaStream_t s) {
@@ -728,6 +971,7 @@ int hive_destroy(hive_table* h) {
         cudaError_t e = cudaFree(h->block);
         if (e != cudaSuccess) rc = cuda_fail(e);
         if (h->defer_q && (e = cudaFree(h->defer_q)) != cudaSuccess) rc = cuda_fail(e);
+        if (h->rbuf && (e = cudaFree(h->rbuf)) != cudaSuccess) rc = cuda_fail(e);
     }
     delete h;
     return rc;
@@ -777,6 +1021,26 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
     Defer d;
     int rc = prepare_defer(h, n, s, &d);
     if (rc) return rc;
+    if (use_regions(h, n)) {
+        // region-ordered: sort, both passes over the sorted arrays, statuses back to caller order
+        Regions r;
+        const int nsub = insert_subbatches(h, n);
+        if ((rc = prepare_regions(h, n, nsub, s, &r)) || (rc = region_sort(h, keys, values, n, r, s))) return rc;
+        for (int k = 0; k < nsub; ++k) {
+            // sub-batch k holds ops i with i * nsub / n == k, i.e. [ceil(k n / nsub), ceil((k+1) n / nsub))
+            const uint64_t lo = ((uint64_t)k * n + nsub - 1) / nsub, hi = ((uint64_t)(k + 1) * n + nsub - 1) / nsub;
+            const uint64_t m = hi - lo;
+            if (!m) continue;
+            if (k && (rc = prepare_defer(h, m, s, &d))) return rc;
+            uint8_t* rst = status ? r.rst + lo : nullptr;
+            HIVE_DISPATCH_D(k_insert, d, grid_for(m), kBlock, s, h->t, r.rkeys + lo, r.rvals + lo, m, rst, d);
+            if (d.q)
+                HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, m), kBlock, s, h->t, r.rkeys + lo, r.rvals + lo, rst,
+                              d);
+        }
+        if (status) k_unpermute_u8<<<grid_for(n), kBlock, 0, s>>>(r.ridx, r.rst, n, status);
+        return launch_check();
+    }
     HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, n, status, d);
     if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, d);
     return launch_check();
@@ -839,7 +1103,16 @@ int hive_find(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* values,
     if (n == 0) return HIVE_OK;
     if (!keys) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
-    HIVE_DISPATCH(k_find, grid_for(n), kBlock, (cudaStream_t)stream, h->t, keys, n, values, found);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (use_regions(h, n)) {
+        Regions r;
+        int rc;
+        if ((rc = prepare_regions(h, n, 1, s, &r)) || (rc = region_sort(h, keys, nullptr, n, r, s))) return rc;
+        HIVE_DISPATCH(k_find, grid_for(n), kBlock, s, h->t, r.rkeys, n, r.rvals, r.rst);
+        k_unpermute_find<<<grid_for(n), kBlock, 0, s>>>(r.ridx, r.rvals, r.rst, n, values, found);
+        return launch_check();
+    }
+    HIVE_DISPATCH(k_find, grid_for(n), kBlock, s, h->t, keys, n, values, found);
     return launch_check();
 }
 
@@ -868,6 +1141,41 @@ int hive_apply_ops(hive_table* h, const uint8_t* types, const uint32_t* keys, co
     if (d.q)
         HIVE_DISPATCH(k_apply_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, out_values, d);
     return launch_check();
+}
+
+int hive_apply_batches(hive_table* h, const uint8_t* types, const uint32_t* keys, const uint32_t* values,
+                       const uint64_t* offsets, uint32_t n_batches, uint64_t max_batch_ops, uint8_t* status,
+                       uint32_t* out_values, uint32_t hints, int threads_per_block, int blocks_per_sm, void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n_batches == 0) return HIVE_OK;
+    if (!types || !keys || !offsets || max_batch_ops == 0 || max_batch_ops > 0xFFFFFFFFull) return HIVE_ERR_INVALID_ARG;
+    if (threads_per_block <= 0) threads_per_block = kBlock;
+    if (threads_per_block % 32 || threads_per_block > 1024 || blocks_per_sm < 0) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
+    Defer d;
+    int rc = prepare_defer(h, max_batch_ops, s, &d);
+    if (rc) return rc;
+    if (!d.q) return HIVE_ERR_INVALID_ARG;
+    HIVE_CUDA(cudaMemsetAsync(h->scratch, 0, 16, s));  // both alternating queue counts
+    const bool holes = h->t.flags & hive::kFlagHoles;
+    const bool p1 = h->policy == HIVE_POLICY_MURMURCITYHASH;
+    const void* fn = p1 ? (holes ? (const void*)k_apply_batches<1, hive::kModeHoles>
+                                 : (const void*)k_apply_batches<1, hive::kModeMono>)
+                        : (holes ? (const void*)k_apply_batches<0, hive::kModeHoles>
+                                 : (const void*)k_apply_batches<0, hive::kModeMono>);
+    int fit = 0;
+    HIVE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, threads_per_block, 0));
+    if (fit < 1) return HIVE_ERR_INVALID_ARG;
+    const int per_sm = blocks_per_sm > 0 ? std::min(blocks_per_sm, fit) : fit;
+    dim3 grid((unsigned)(per_sm * h->num_sms)), block((unsigned)threads_per_block);
+    hive::Table tv = h->t;
+    u64* qn = h->scratch;  // two counts: scratch[0], scratch[1]
+    void* args[] = {(void*)&tv, (void*)&types, (void*)&keys, (void*)&values, (void*)&offsets, (void*)&n_batches,
+                    (void*)&status, (void*)&out_values, (void*)&d.q, (void*)&qn};
+    HIVE_CUDA(cudaLaunchCooperativeKernel(fn, grid, block, args, 0, s));
+    return HIVE_OK;
 }
 
 int hive_apply_reference_ops(hive_table* h, const void* ops, uint64_t n, uint64_t* results, uint32_t hints,

@@ -80,6 +80,7 @@ ABI = [
     ("hive_erase", _I32, [_P, _P, _U64, _P, _P]),
     ("hive_apply_ops", _I32, [_P, _P, _P, _P, _U64, _P, _P, _U32, _P]),
     ("hive_apply_reference_ops", _I32, [_P, _P, _U64, _P, _U32, _P]),
+    ("hive_apply_batches", _I32, [_P, _P, _P, _P, _P, _U32, _U64, _P, _P, _U32, _I32, _I32, _P]),
     ("hive_size", _I32, [_P, ctypes.POINTER(_U64), _P]),
     ("hive_dump", _I32, [_P, _P, _U64, ctypes.POINTER(_U64), _P]),
     ("hive_resize", _I32, [_P, _U64, _P]),
@@ -245,6 +246,17 @@ class HiveHashTable:
         _check(self._lib.hive_apply_ops(self._h, _ptr(t), _ptr(k), _ptr(v), n, _ptr(status), _ptr(outv),
                                         hints, self._stream(stream)), "hive_apply_ops")
         return status, outv
+
+    def apply_batches(self, types: torch.Tensor, keys: torch.Tensor, values: Optional[torch.Tensor],
+                      offsets: torch.Tensor, max_batch_ops: int, status: torch.Tensor, out_values: torch.Tensor,
+                      hints: int = 0, threads_per_block: int = 256, blocks_per_sm: int = 0, stream=None) -> None:
+        """Batches [offsets[b], offsets[b+1]) of device op arrays in one persistent launch
+        (hive_apply_batches); outputs are written into status / out_values at global positions."""
+        nb = offsets.numel() - 1
+        _check(self._lib.hive_apply_batches(self._h, _ptr(types), _ptr(keys), _ptr(values), _ptr(offsets), nb,
+                                            int(max_batch_ops), _ptr(status), _ptr(out_values), hints,
+                                            threads_per_block, blocks_per_sm, self._stream(stream)),
+               "hive_apply_batches")
 
     def apply_reference_ops(self, ops: torch.Tensor, hints: int = 0, stream=None) -> torch.Tensor:
         """ops: int64 tensor of shape (n, 2) holding the reference's 16-byte Operation records

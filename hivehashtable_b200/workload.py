@@ -38,6 +38,11 @@ def lib() -> ctypes.CDLL:
         L.hive_wl_shuffle.argtypes = [P, U64, ctypes.POINTER(U64)]
         L.hive_wl_lookup_set.restype = None
         L.hive_wl_lookup_set.argtypes = [P, U64, P, U64, U64, ctypes.POINTER(U64), P]
+        D = ctypes.c_double
+        L.hive_wl_mixed_plan.restype = U64
+        L.hive_wl_mixed_plan.argtypes = [U64, U64, D, D, P]
+        L.hive_wl_mixed_fill.restype = U64
+        L.hive_wl_mixed_fill.argtypes = [U64, U64, U64, D, D, P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -94,3 +99,37 @@ def bulk_workload(seed: int, n: int, present_fraction: float, n_lookups: int | N
     vals = values_for(keys)
     lk, _ = lookup_set(keys, absent, n_present, n_absent, state)
     return keys, vals, lk
+
+
+class MixedWorkload:
+    """Prefill keys and a sequence of mixed batches (csrc/hive_workload.cpp, hive_wl_mixed_fill):
+    each batch is 50 % inserts of new keys, 40 % lookups (80 % of live keys), 10 % deletes of live
+    keys, at most one op per key per batch, sizes floor(2^U) with U uniform in [log_lo, log_hi)."""
+
+    def __init__(self, seed: int, prefill: int, n_batches: int, log_lo: float = 10.0, log_hi: float = 20.0):
+        L = lib()
+        sizes = np.empty(n_batches, dtype=np.uint64)
+        total = L.hive_wl_mixed_plan(seed, n_batches, log_lo, log_hi, _p(sizes))
+        self.prefill_keys = np.empty(prefill, dtype=np.uint32)
+        self.types = np.empty(total, dtype=np.uint8)
+        self.keys = np.empty(total, dtype=np.uint32)
+        self.vals = np.empty(total, dtype=np.uint32)
+        self.offsets = np.empty(n_batches + 1, dtype=np.uint64)
+        self.final_live = int(L.hive_wl_mixed_fill(seed, prefill, n_batches, log_lo, log_hi, _p(self.prefill_keys),
+                                                   _p(self.types), _p(self.keys), _p(self.vals), _p(self.offsets)))
+        self.prefill_vals = values_for(self.prefill_keys)
+        self.seed, self.n_batches = seed, n_batches
+
+    @property
+    def total_ops(self) -> int:
+        return int(self.offsets[-1])
+
+    def batch(self, b: int):
+        lo, hi = int(self.offsets[b]), int(self.offsets[b + 1])
+        return self.types[lo:hi], self.keys[lo:hi], self.vals[lo:hi]
+
+    def live_after(self) -> np.ndarray:
+        """Live-key count after each batch (prefill + inserts - deletes so far)."""
+        ins = np.add.reduceat((self.types == 0).astype(np.int64), self.offsets[:-1].astype(np.int64))
+        dels = np.add.reduceat((self.types == 2).astype(np.int64), self.offsets[:-1].astype(np.int64))
+        return self.prefill_keys.size + np.cumsum(ins - dels)

@@ -159,6 +159,19 @@ int hive_erase(hive_table* t, const uint32_t* keys, uint64_t n, uint8_t* status,
 int hive_apply_ops(hive_table* t, const uint8_t* types, const uint32_t* keys, const uint32_t* values,
                    uint64_t n, uint8_t* status, uint32_t* out_values, uint32_t hints, void* stream);
 
+/* A sequence of mixed batches in ONE persistent (cooperative) launch: batch b is ops
+ * [offsets[b], offsets[b+1]) of types/keys/values (device arrays, offsets a device array of
+ * n_batches + 1 entries); ops within a batch are unordered, batches are applied in order (a grid
+ * barrier separates them).  Outputs as hive_apply_ops, indexed by global op position.
+ * max_batch_ops >= the largest batch.  blocks_per_sm: 0 = as many as fit.  The table geometry is
+ * fixed for the launch: grow it (hive_resize) before a sequence that would overfill it.
+ * Replaces the reference's host loop of one hive_mixed_kernel launch per batch
+ * (src/hive_dispatch.cu:119-226) with one launch per sequence. */
+int hive_apply_batches(hive_table* t, const uint8_t* types, const uint32_t* keys, const uint32_t* values,
+                       const uint64_t* offsets, uint32_t n_batches, uint64_t max_batch_ops, uint8_t* status,
+                       uint32_t* out_values, uint32_t hints, int threads_per_block, int blocks_per_sm,
+                       void* stream);
+
 /* Mixed batch in the reference's own record layout: ops points to n 16-byte records
  * {int32 type (OperationType); 4 bytes padding; uint64 key} (include/utils.h:18-21);
  * value = (uint32)key + 1 (include/hive_kernels.cuh:156); results[i] = 1 on success else 0,
