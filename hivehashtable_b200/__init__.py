@@ -21,6 +21,7 @@ from .table import (  # noqa: F401
     HiveError,
     HiveHashTable,
     as_device_u32,
+    as_host_u32,
     library,
     u32,
 )

@@ -19,7 +19,8 @@
 //                                evictor reads it for all 8 victims' alternate buckets at once
 //                                (L2 hits) and then reads just one bucket that has room, where
 //                                the reference probes victims' buckets one by one
-//   counters   u64[16]           slow-path event counters and the sticky error word
+//   counters   u64[64 * 16]      slow-path event counters in 64 stripes of 16 words (summed by
+//                                the host) and the sticky error word (stripe 0, word 15)
 //
 // A slot holds (value << 32) | key (include/hive_hash_table_struct.cuh:297-311); key 0 is the
 // empty sentinel, so an all-zero slot is free (include/utils.h:39-47).  There is no freeMask
@@ -241,7 +242,30 @@ __device__ __forceinline__ bool stash_flag_ro(const Table& t, uint32_t b) {
     return (__ldg(t.stash_bits + (b >> 5)) >> (b & 31)) & 1u;
 }
 
-__device__ __forceinline__ void count(const Table& t, int ctr) { atomicAdd(t.counters + ctr, 1ull); }
+// Event counters are striped: stripe s (s = SM id mod kCounterStripes) holds its own 16 words,
+// 128 B apart, and the host sums the stripes.  One shared word would serialise every slow-path
+// op of a launch on one L2 slice (millions of same-address atomics at about one per clock).
+// Within a warp, the lanes counting the same event add their count with one atomic.
+constexpr int kCounterStripes = 64;
+constexpr int kCounterStride = 16;  // u64 words per stripe
+
+__device__ __forceinline__ unsigned sm_id() {
+    unsigned id;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(id));
+    return id;
+}
+__device__ __forceinline__ unsigned lane_id() {
+    unsigned id;
+    asm volatile("mov.u32 %0, %%laneid;" : "=r"(id));
+    return id;
+}
+
+__device__ __forceinline__ void count(const Table& t, int ctr) {
+    const unsigned peers = __match_any_sync(__activemask(), ctr);
+    if (lane_id() == (unsigned)(__ffs(peers) - 1))
+        atomicAdd(t.counters + (sm_id() % kCounterStripes) * kCounterStride + ctr, (u64)__popc(peers));
+}
+// The sticky error word lives in stripe 0 only.
 __device__ __forceinline__ void raise_error(const Table& t, u64 bits) { atomicOr(t.counters + kCtrError, bits); }
 
 // Full-bucket hints.  mark_full is called by the claim that took a bucket's last free slot.
@@ -573,15 +597,18 @@ __device__ __forceinline__ uint8_t claim_or_update(const Table& t, uint32_t b, u
 
 // Which insert protocol a kernel compiles: chosen from the table's flags at run time, or fixed
 // by the host (which knows the flags) so the kernel carries only the code it needs.
-enum Mode { kModeRuntime = 0, kModeMono = 1, kModeHoles = 2 };
+// kModeMonoPrimary is kModeMono whose deferring first pass claims in H0 only (region-ordered
+// batches, see insert_lockfree).
+enum Mode { kModeRuntime = 0, kModeMono = 1, kModeHoles = 2, kModeMonoPrimary = 3 };
 
 // Lock-free stages A and B.  Returns the op's final status, or 0 when the op must go on: to the
 // locked path (stages C/D) when H0 and H1 are both full, or -- with kPrimaryOnly, the first pass
-// of a two-pass insert -- as soon as H0 is full.  Claiming only in H0 in the first pass and
-// leaving every claim in H1 to the second pass fills the table primary-first: no key's overflow
-// takes an H0 slot that one of that bucket's own keys would claim later in the same batch.  This
-// keeps the final placement independent of the order the batch is processed in (including the
-// region order of large batches) and leaves more keys in H0, where lookups find them first.
+// of a region-ordered insert -- as soon as H0 is full.  A region-ordered batch reaches the
+// buckets in address order, so a first pass that claimed in H1 would let the early regions'
+// overflow take the H1 slots that later regions' own keys need; claiming only in H0 there and
+// leaving every H1 claim to the second pass keeps the placement independent of the region order.
+// In submission order (the default) the first pass claims in H0, then in H1: overflow then meets
+// a table that is still filling, and fewer ops reach eviction and the stash.
 template <int P, int kMode = kModeRuntime, bool kPrimaryOnly = false>
 __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
     u64* B0p = t.slots + (size_t)b0 * kSlots;
@@ -653,7 +680,7 @@ __device__ __forceinline__ uint8_t insert_one(const Table& t, uint32_t k, uint32
     const u64 kv = pack(k, v);
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
     const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
-    uint8_t st = insert_lockfree<P, kMode, kDefer>(t, k, kv, b0, b1);
+    uint8_t st = insert_lockfree<P, kMode, kDefer && kMode == kModeMonoPrimary>(t, k, kv, b0, b1);
     if (st) return st;
     if (kDefer) return kStDefer;
     return insert_locked_path<P>(t, k, kv, b0, b1);

@@ -75,6 +75,13 @@ struct hive_table {
     void* rbuf = nullptr;         // region-ordering buffers (13 bytes per op of the largest batch)
     uint64_t rcap = 0;
     int num_sms = 148;
+    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4};  // HIVE_TUNE_* knobs
+    // host-buffer pipeline (hive_insert_host / hive_find_host): copy streams, events and device
+    // staging arrays (insert keys, values, statuses; find keys, values, flags: 18 bytes per op)
+    cudaStream_t pipe_h2d = nullptr, pipe_d2h = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_ins_free = nullptr, ev_find_free = nullptr;
+    void* hbuf = nullptr;
+    uint64_t hcap = 0;
 };
 
 namespace {
@@ -91,6 +98,9 @@ void set_geometry(hive_table* h, uint32_t level, uint32_t split) {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+constexpr size_t kCounterBytes = (size_t)hive::kCounterStripes * hive::kCounterStride * 8;
+static_assert(hive::kCounterStride >= HIVE_NUM_COUNTERS, "a counter stripe holds every counter");
+
 struct Carve {
     size_t slots, stash, sbits, lbits, fbits, ctr, scratch, total;
 };
@@ -103,7 +113,7 @@ Carve carve(uint64_t nb_cap) {
     c.lbits = align256(c.sbits + words * 4);
     c.fbits = align256(c.lbits + (size_t)nb_cap * 4);
     c.ctr = align256(c.fbits + words * 4);
-    c.scratch = align256(c.ctr + HIVE_NUM_COUNTERS * 8);
+    c.scratch = align256(c.ctr + kCounterBytes);
     c.total = align256(c.scratch + 16);
     return c;
 }
@@ -155,13 +165,15 @@ __device__ __forceinline__ void defer_push(const Defer& d, bool deferred, uint64
     if (deferred) d.q[base + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
 }
 
-// First pass (kDefer) or the whole protocol in one pass (!kDefer, batches too large to queue).
+// First pass (kDefer) or the whole protocol in one pass (!kDefer, batches too large to queue)
+// over ops [lo, hi) of the batch; deferred ops are queued by their index in the batch, so the
+// first passes of several chunks of one batch feed one second pass.
 template <int P, bool kDefer, int kMode>
-__global__ void __launch_bounds__(kBlock, (kDefer && kMode == hive::kModeMono) ? 8 : 1) k_insert(hive::Table t, const uint32_t* __restrict__ keys,
-                                                   const uint32_t* __restrict__ vals, uint64_t n,
-                                                   uint8_t* __restrict__ status, Defer d) {
-    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
-    const bool active = i < n;
+__global__ void __launch_bounds__(kBlock, (kDefer && (kMode == hive::kModeMono || kMode == hive::kModeMonoPrimary)) ? 8 : 1)
+    k_insert(hive::Table t, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, uint64_t lo,
+             uint64_t hi, uint8_t* __restrict__ status, Defer d) {
+    const uint64_t i = lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < hi;
     uint8_t st = hive::kStFail;
     if (active) st = hive::insert_one<P, kDefer, kMode>(t, __ldcs(keys + i), __ldcs(vals + i));
     if (kDefer) defer_push(d, st == hive::kStDefer, i);
@@ -694,7 +706,7 @@ int reset(hive_table* h, cudaStream_t s) {
     HIVE_CUDA(cudaMemsetAsync(h->t.stash_bits, 0, (size_t)words * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.locks, 0, (size_t)nb * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.full_bits, 0, (size_t)words * 4, s));
-    HIVE_CUDA(cudaMemsetAsync(h->t.counters, 0, HIVE_NUM_COUNTERS * 8, s));
+    HIVE_CUDA(cudaMemsetAsync(h->t.counters, 0, kCounterBytes, s));
     return HIVE_OK;
 }
 
@@ -720,7 +732,7 @@ int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d) {
 }
 
 unsigned second_pass_grid(const hive_table* h, uint64_t n) {
-    return (unsigned)std::min<uint64_t>(grid_for(n), (uint64_t)h->num_sms * 4);
+    return (unsigned)std::min<uint64_t>(grid_for(n), (uint64_t)h->num_sms * h->tune[HIVE_TUNE_SECOND_PASS_BLOCKS]);
 }
 
 // Region ordering pays off when the batch touches each bucket about once or more and the table
@@ -733,9 +745,10 @@ struct Regions {
     uint8_t* rst = nullptr;
 };
 
-bool use_regions(const hive_table* h, uint64_t n) {
+// `knob` = HIVE_TUNE_REGION_INSERT or HIVE_TUNE_REGION_FIND.
+bool use_regions(const hive_table* h, uint64_t n, int knob) {
     const uint64_t nb = num_buckets(h);
-    return nb >= kRegionMinBuckets && n >= nb && n <= 0xFFFFFFFFull;
+    return h->tune[knob] && nb >= kRegionMinBuckets && n >= nb && n <= 0xFFFFFFFFull;
 }
 
 // Geometry and buffers of the region ordering for a batch of n ops; the buffers grow
@@ -772,6 +785,7 @@ int prepare_regions(hive_table* h, uint64_t n, int nsub, cudaStream_t s, Regions
 // Sub-batches for a region-ordered insert of n ops: more when the batch adds a larger share of
 // the table's capacity (see region_bin).
 int insert_subbatches(const hive_table* h, uint64_t n) {
+    if (h->tune[HIVE_TUNE_SUBBATCHES]) return (int)h->tune[HIVE_TUNE_SUBBATCHES];
     const double share = (double)n / (double)(num_buckets(h) * hive::kSlots);
     return share <= 0.25 ? 1 : share <= 0.5 ? 2 : share <= 0.75 ? 4 : 8;
 }
@@ -818,7 +832,7 @@ int grow_capacity(hive_table* h, uint64_t need_buckets, cudaStream_t s) {
             cudaSuccess ||
         (e = cudaMemcpyAsync(nbase + c.fbits, obase + oc.fbits, owords * 4, cudaMemcpyDeviceToDevice, s)) !=
             cudaSuccess ||
-        (e = cudaMemcpyAsync(nbase + c.ctr, obase + oc.ctr, HIVE_NUM_COUNTERS * 8, cudaMemcpyDeviceToDevice, s)) !=
+        (e = cudaMemcpyAsync(nbase + c.ctr, obase + oc.ctr, kCounterBytes, cudaMemcpyDeviceToDevice, s)) !=
             cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess) {
         cudaFree(nblock);
@@ -972,6 +986,11 @@ int hive_destroy(hive_table* h) {
         if (e != cudaSuccess) rc = cuda_fail(e);
         if (h->defer_q && (e = cudaFree(h->defer_q)) != cudaSuccess) rc = cuda_fail(e);
         if (h->rbuf && (e = cudaFree(h->rbuf)) != cudaSuccess) rc = cuda_fail(e);
+        if (h->hbuf && (e = cudaFree(h->hbuf)) != cudaSuccess) rc = cuda_fail(e);
+        for (cudaEvent_t ev : {h->ev_in, h->ev_out, h->ev_ins_free, h->ev_find_free})
+            if (ev) cudaEventDestroy(ev);
+        for (cudaStream_t st : {h->pipe_h2d, h->pipe_d2h})
+            if (st) cudaStreamDestroy(st);
     }
     delete h;
     return rc;
@@ -995,13 +1014,16 @@ int hive_clear(hive_table* h, void* stream) {
     } while (0)
 
 // Launch a two-pass kernel: the first pass with deferral when the queue exists, else one pass.
-#define HIVE_DISPATCH_D(kern, d, grid, block, stream, ...)                                  \
+// HIVE_DISPATCH_DM names the mode of a deferring first pass on a table without holes.
+#define HIVE_DISPATCH_D(kern, d, grid, block, stream, ...) \
+    HIVE_DISPATCH_DM(kern, hive::kModeMono, d, grid, block, stream, __VA_ARGS__)
+#define HIVE_DISPATCH_DM(kern, mono, d, grid, block, stream, ...)                            \
     do {                                                                                   \
         const bool p1_ = h->policy == HIVE_POLICY_MURMURCITYHASH;                          \
         const bool holes_ = h->t.flags & hive::kFlagHoles;                                 \
         if (d.q && !holes_) {                                                              \
-            if (p1_) kern<1, true, hive::kModeMono><<<grid, block, 0, stream>>>(__VA_ARGS__);  \
-            else kern<0, true, hive::kModeMono><<<grid, block, 0, stream>>>(__VA_ARGS__);      \
+            if (p1_) kern<1, true, mono><<<grid, block, 0, stream>>>(__VA_ARGS__);             \
+            else kern<0, true, mono><<<grid, block, 0, stream>>>(__VA_ARGS__);                 \
         } else if (d.q) {                                                                  \
             if (p1_) kern<1, true, hive::kModeHoles><<<grid, block, 0, stream>>>(__VA_ARGS__); \
             else kern<0, true, hive::kModeHoles><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
@@ -1021,7 +1043,7 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
     Defer d;
     int rc = prepare_defer(h, n, s, &d);
     if (rc) return rc;
-    if (use_regions(h, n)) {
+    if (use_regions(h, n, HIVE_TUNE_REGION_INSERT)) {
         // region-ordered: sort, both passes over the sorted arrays, statuses back to caller order
         Regions r;
         const int nsub = insert_subbatches(h, n);
@@ -1033,7 +1055,8 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
             if (!m) continue;
             if (k && (rc = prepare_defer(h, m, s, &d))) return rc;
             uint8_t* rst = status ? r.rst + lo : nullptr;
-            HIVE_DISPATCH_D(k_insert, d, grid_for(m), kBlock, s, h->t, r.rkeys + lo, r.rvals + lo, m, rst, d);
+            HIVE_DISPATCH_DM(k_insert, hive::kModeMonoPrimary, d, grid_for(m), kBlock, s, h->t, r.rkeys + lo, r.rvals + lo,
+                             0, m, rst, d);
             if (d.q)
                 HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, m), kBlock, s, h->t, r.rkeys + lo, r.rvals + lo, rst,
                               d);
@@ -1041,7 +1064,7 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
         if (status) k_unpermute_u8<<<grid_for(n), kBlock, 0, s>>>(r.ridx, r.rst, n, status);
         return launch_check();
     }
-    HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, n, status, d);
+    HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, 0, n, status, d);
     if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, d);
     return launch_check();
 }
@@ -1093,7 +1116,7 @@ int hive_insert_noalloc(hive_table* h, const uint32_t* keys, const uint32_t* val
     cudaStream_t s = (cudaStream_t)stream;
     Defer d{base + kNoAllocHeaderWords, (u64*)base};
     HIVE_CUDA(cudaMemsetAsync(d.n, 0, sizeof(u64), s));  // the queue count must start at zero
-    HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, n, status, d);
+    HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, 0, n, status, d);
     HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, d);
     return launch_check();
 }
@@ -1104,7 +1127,7 @@ int hive_find(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* values,
     if (!keys) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
-    if (use_regions(h, n)) {
+    if (use_regions(h, n, HIVE_TUNE_REGION_FIND)) {
         Regions r;
         int rc;
         if ((rc = prepare_regions(h, n, 1, s, &r)) || (rc = region_sort(h, keys, nullptr, n, r, s))) return rc;
@@ -1113,6 +1136,116 @@ int hive_find(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* values,
         return launch_check();
     }
     HIVE_DISPATCH(k_find, grid_for(n), kBlock, s, h->t, keys, n, values, found);
+    return launch_check();
+}
+
+}  // extern "C"
+
+// ---- host-buffer pipeline ------------------------------------------------------------------------
+// A batch in host memory is copied in chunks on a copy stream and each chunk is processed on the
+// caller's stream as soon as it has landed, so PCIe transfers overlap the table work; results go
+// back on a second copy stream (PCIe is full duplex).  The caller's stream waits for the last
+// copy, so synchronising it covers the whole call.  The device staging arrays of a kind (insert
+// or find) are reused by the next call of that kind only after this call has finished with them
+// (ev_ins_free / ev_find_free), which lets a find's key upload run while an insert is computing.
+namespace {
+constexpr uint64_t kPipeChunk = 1ull << 22;  // ops per chunk: 16 MiB of keys
+
+struct Staging {
+    uint32_t *ik, *iv, *fk, *fv;
+    uint8_t *ist, *ff;
+};
+
+int prepare_pipe(hive_table* h, uint64_t n, Staging* st) {
+    if (!h->pipe_h2d) {
+        HIVE_CUDA(cudaStreamCreateWithFlags(&h->pipe_h2d, cudaStreamNonBlocking));
+        HIVE_CUDA(cudaStreamCreateWithFlags(&h->pipe_d2h, cudaStreamNonBlocking));
+        for (cudaEvent_t* ev : {&h->ev_in, &h->ev_out, &h->ev_ins_free, &h->ev_find_free})
+            HIVE_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    }
+    if (n > h->hcap) {
+        HIVE_CUDA(cudaDeviceSynchronize());
+        if (h->hbuf) cudaFree(h->hbuf);
+        h->hbuf = nullptr;
+        h->hcap = 0;
+        cudaError_t e = cudaMalloc(&h->hbuf, align256((size_t)n * 4) * 4 + align256((size_t)n) * 2);
+        if (e != cudaSuccess) return cuda_fail(e);
+        h->hcap = n;
+    }
+    const size_t w = align256((size_t)h->hcap * 4), b = align256((size_t)h->hcap);
+    char* p = (char*)h->hbuf;
+    st->ik = (uint32_t*)p;
+    st->iv = (uint32_t*)(p + w);
+    st->fk = (uint32_t*)(p + 2 * w);
+    st->fv = (uint32_t*)(p + 3 * w);
+    st->ist = (uint8_t*)(p + 4 * w);
+    st->ff = (uint8_t*)(p + 4 * w + b);
+    return HIVE_OK;
+}
+
+// `after` waits for everything issued so far on `before`.
+cudaError_t order(cudaEvent_t ev, cudaStream_t before, cudaStream_t after) {
+    cudaError_t e = cudaEventRecord(ev, before);
+    return e == cudaSuccess ? cudaStreamWaitEvent(after, ev, 0) : e;
+}
+}  // namespace
+
+extern "C" {
+
+int hive_insert_host(hive_table* h, const uint32_t* keys, const uint32_t* values, uint64_t n, uint8_t* status,
+                     void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n == 0) return HIVE_OK;
+    if (!keys || !values) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    if (!g.ok) return HIVE_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    Staging st;
+    Defer d;
+    int rc;
+    if ((rc = prepare_pipe(h, n, &st)) || (rc = prepare_defer(h, n, s, &d))) return rc;
+    HIVE_CUDA(cudaStreamWaitEvent(h->pipe_h2d, h->ev_ins_free, 0));
+    uint8_t* dst = status ? st.ist : nullptr;
+    for (uint64_t lo = 0; lo < n; lo += kPipeChunk) {
+        const uint64_t m = std::min(kPipeChunk, n - lo);
+        HIVE_CUDA(cudaMemcpyAsync(st.ik + lo, keys + lo, m * 4, cudaMemcpyHostToDevice, h->pipe_h2d));
+        HIVE_CUDA(cudaMemcpyAsync(st.iv + lo, values + lo, m * 4, cudaMemcpyHostToDevice, h->pipe_h2d));
+        HIVE_CUDA(order(h->ev_in, h->pipe_h2d, s));
+        // first pass of this chunk; its deferred ops join the batch's one queue
+        HIVE_DISPATCH_D(k_insert, d, grid_for(m), kBlock, s, h->t, st.ik, st.iv, lo, lo + m, dst, d);
+    }
+    if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, st.ik, st.iv, dst, d);
+    if (status) {
+        HIVE_CUDA(order(h->ev_out, s, h->pipe_d2h));
+        HIVE_CUDA(cudaMemcpyAsync(status, st.ist, n, cudaMemcpyDeviceToHost, h->pipe_d2h));
+        HIVE_CUDA(order(h->ev_out, h->pipe_d2h, s));
+    }
+    HIVE_CUDA(cudaEventRecord(h->ev_ins_free, s));
+    return launch_check();
+}
+
+int hive_find_host(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* values, uint8_t* found, void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n == 0) return HIVE_OK;
+    if (!keys) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    if (!g.ok) return HIVE_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    Staging st;
+    int rc = prepare_pipe(h, n, &st);
+    if (rc) return rc;
+    HIVE_CUDA(cudaStreamWaitEvent(h->pipe_h2d, h->ev_find_free, 0));
+    for (uint64_t lo = 0; lo < n; lo += kPipeChunk) {
+        const uint64_t m = std::min(kPipeChunk, n - lo);
+        HIVE_CUDA(cudaMemcpyAsync(st.fk + lo, keys + lo, m * 4, cudaMemcpyHostToDevice, h->pipe_h2d));
+        HIVE_CUDA(order(h->ev_in, h->pipe_h2d, s));
+        HIVE_DISPATCH(k_find, grid_for(m), kBlock, s, h->t, st.fk + lo, m, st.fv + lo, st.ff + lo);
+        if (values || found) HIVE_CUDA(order(h->ev_out, s, h->pipe_d2h));
+        if (values) HIVE_CUDA(cudaMemcpyAsync(values + lo, st.fv + lo, m * 4, cudaMemcpyDeviceToHost, h->pipe_d2h));
+        if (found) HIVE_CUDA(cudaMemcpyAsync(found + lo, st.ff + lo, m, cudaMemcpyDeviceToHost, h->pipe_d2h));
+    }
+    HIVE_CUDA(order(h->ev_out, h->pipe_d2h, s));
+    HIVE_CUDA(cudaEventRecord(h->ev_find_free, s));
     return launch_check();
 }
 
@@ -1284,8 +1417,29 @@ int hive_counters(hive_table* h, uint64_t* out, void* stream) {
     if (!valid_table(h) || !out) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
-    HIVE_CUDA(cudaMemcpyAsync(out, h->t.counters, HIVE_NUM_COUNTERS * 8, cudaMemcpyDeviceToHost, s));
+    uint64_t stripes[hive::kCounterStripes * hive::kCounterStride];
+    HIVE_CUDA(cudaMemcpyAsync(stripes, h->t.counters, kCounterBytes, cudaMemcpyDeviceToHost, s));
     HIVE_CUDA(cudaStreamSynchronize(s));
+    for (int c = 0; c < HIVE_NUM_COUNTERS; ++c) {
+        uint64_t v = 0;
+        for (int k = 0; k < hive::kCounterStripes; ++k)
+            v = c == HIVE_CTR_ERROR ? v | stripes[k * hive::kCounterStride + c] : v + stripes[k * hive::kCounterStride + c];
+        out[c] = v;
+    }
+    return HIVE_OK;
+}
+
+int hive_set_tuning(hive_table* h, int32_t key, int64_t value) {
+    if (!valid_table(h) || key < 0 || key >= HIVE_NUM_TUNES) return HIVE_ERR_INVALID_ARG;
+    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1}, hi[HIVE_NUM_TUNES] = {1, 1, 8, 8};
+    if (value < lo[key] || value > hi[key]) return HIVE_ERR_INVALID_ARG;
+    h->tune[key] = value;
+    return HIVE_OK;
+}
+
+int hive_get_tuning(const hive_table* h, int32_t key, int64_t* value) {
+    if (!valid_table(h) || !value || key < 0 || key >= HIVE_NUM_TUNES) return HIVE_ERR_INVALID_ARG;
+    *value = h->tune[key];
     return HIVE_OK;
 }
 

@@ -36,6 +36,8 @@ HINT_NO_DELETES = 1
 NUM_COUNTERS = 16
 COUNTER_NAMES = {0: "slow_path", 1: "evictions", 2: "stash_push", 3: "failed", 4: "lock_timeout",
                  5: "retry_out", 6: "dup_fixed", 15: "error_bits"}
+# Launch-tuning knobs (HIVE_TUNE_*): how a batch runs, never what it computes
+TUNES = {"region_insert": 0, "region_find": 1, "subbatches": 2, "second_pass_blocks": 3}
 
 # Policy names accepted by the reference's dispatcher (src/hive_dispatch.cu:829-871).  The
 # ones outside the hot path fall back to Default2Hash with a message, as the reference does for
@@ -77,6 +79,8 @@ ABI = [
     ("hive_insert", _I32, [_P, _P, _P, _U64, _P, _P]),
     ("hive_insert_noalloc", _I32, [_P, _P, _P, _U64, _P, _P]),
     ("hive_find", _I32, [_P, _P, _U64, _P, _P, _P]),
+    ("hive_insert_host", _I32, [_P, _P, _P, _U64, _P, _P]),
+    ("hive_find_host", _I32, [_P, _P, _U64, _P, _P, _P]),
     ("hive_erase", _I32, [_P, _P, _U64, _P, _P]),
     ("hive_apply_ops", _I32, [_P, _P, _P, _P, _U64, _P, _P, _U32, _P]),
     ("hive_apply_reference_ops", _I32, [_P, _P, _U64, _P, _U32, _P]),
@@ -88,6 +92,8 @@ ABI = [
     ("hive_get_info", _I32, [_P, ctypes.POINTER(Info)]),
     ("hive_counters", _I32, [_P, _P, _P]),
     ("hive_check", _I32, [_P, _P]),
+    ("hive_set_tuning", _I32, [_P, _I32, ctypes.c_int64]),
+    ("hive_get_tuning", _I32, [_P, _I32, ctypes.POINTER(ctypes.c_int64)]),
     ("hive_strerror", ctypes.c_char_p, [_I32]),
     ("hive_last_cuda_error", _I32, []),
 ]
@@ -145,6 +151,18 @@ def as_device_u8(x, device: torch.device) -> torch.Tensor:
     return torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.uint8))).to(device)
 
 
+def as_host_u32(x) -> torch.Tensor:
+    """A contiguous 4-byte CPU tensor holding the uint32 bit patterns of x (no copy when x already
+    is one, so a page-locked tensor stays page-locked)."""
+    if isinstance(x, torch.Tensor):
+        if x.device.type != "cpu":
+            raise ValueError("host-buffer calls take CPU tensors or numpy arrays")
+        if x.element_size() != 4:
+            x = x.to(torch.int64).to(torch.int32)
+        return (x.view(torch.int32) if x.dtype != torch.int32 else x).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.uint32)).view(np.int32))
+
+
 def u32(t: torch.Tensor) -> np.ndarray:
     """Device int32 tensor -> host numpy uint32 (bit pattern preserved)."""
     return t.cpu().numpy().view(np.uint32)
@@ -183,6 +201,9 @@ class HiveHashTable:
     def _stream(self, stream=None) -> int:
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         return s.cuda_stream
+
+    def _sync(self, stream=None) -> None:
+        (stream if stream is not None else torch.cuda.current_stream(self.device)).synchronize()
 
     @property
     def handle(self) -> int:
@@ -226,6 +247,38 @@ class HiveHashTable:
             found = torch.empty(k.numel(), dtype=torch.uint8, device=self.device)
         _check(self._lib.hive_find(self._h, _ptr(k), k.numel(), _ptr(values), _ptr(found),
                                    self._stream(stream)), "hive_find")
+        return values, found
+
+    def insert_host(self, keys, values, status: Optional[torch.Tensor] = None, stream=None,
+                    sync: bool = True) -> torch.Tensor:
+        """insert() from host memory with the copies overlapped with the work (hive_insert_host).
+        Pass page-locked CPU tensors (and a page-locked `status`) for overlap.  With sync=False
+        the call returns once queued: inputs and `status` belong to it until `stream` completes."""
+        k, v = as_host_u32(keys), as_host_u32(values)
+        if k.numel() != v.numel():
+            raise ValueError("keys and values differ in length")
+        if status is None:
+            status = torch.empty(k.numel(), dtype=torch.uint8)
+        s = self._stream(stream)
+        _check(self._lib.hive_insert_host(self._h, _ptr(k), _ptr(v), k.numel(), _ptr(status), s),
+               "hive_insert_host")
+        if sync:
+            self._sync(stream)
+        return status
+
+    def find_host(self, keys, values: Optional[torch.Tensor] = None, found: Optional[torch.Tensor] = None,
+                  stream=None, sync: bool = True) -> Tuple[torch.Tensor, torch.Tensor]:
+        """find() from host memory (hive_find_host); same rules as insert_host."""
+        k = as_host_u32(keys)
+        if values is None:
+            values = torch.empty(k.numel(), dtype=torch.int32)
+        if found is None:
+            found = torch.empty(k.numel(), dtype=torch.uint8)
+        s = self._stream(stream)
+        _check(self._lib.hive_find_host(self._h, _ptr(k), k.numel(), _ptr(values), _ptr(found), s),
+               "hive_find_host")
+        if sync:
+            self._sync(stream)
         return values, found
 
     def erase(self, keys, status: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
@@ -316,6 +369,19 @@ class HiveHashTable:
 
     def check(self, stream=None) -> None:
         _check(self._lib.hive_check(self._h, self._stream(stream)), "hive_check")
+
+    def set_tuning(self, **knobs) -> None:
+        """set_tuning(region_insert=1, subbatches=4, ...): see TUNES."""
+        for name, value in knobs.items():
+            _check(self._lib.hive_set_tuning(self._h, TUNES[name], int(value)), f"hive_set_tuning({name})")
+
+    def tuning(self) -> dict:
+        out = {}
+        for name, key in TUNES.items():
+            v = ctypes.c_int64()
+            _check(self._lib.hive_get_tuning(self._h, key, ctypes.byref(v)), "hive_get_tuning")
+            out[name] = v.value
+        return out
 
     def load_factor(self) -> float:
         return self.size() / self.info()["capacity_slots"]

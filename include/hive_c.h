@@ -140,6 +140,23 @@ int hive_insert(hive_table* t, const uint32_t* keys, const uint32_t* values, uin
 int hive_insert_noalloc(hive_table* t, const uint32_t* keys, const uint32_t* values, uint64_t n,
                         uint8_t* status, void* stream);
 
+/* hive_insert with keys, values and status in HOST memory (page-locked for overlap; pageable
+ * works but its copies do not overlap).  The batch is copied in chunks of 2^22 ops on an internal
+ * copy stream and each chunk's first pass runs on `stream` as soon as it lands; one second pass
+ * finishes the batch and the statuses are copied back on a second copy stream, so the result
+ * equals hive_insert's on the same batch.  Returns once the work is queued; `status` and the
+ * inputs belong to the call until `stream` completes.  Device staging arrays (18 bytes per op
+ * of the largest host batch) are kept by the table.  Replaces the host-side steps of
+ * hash_table_kernel_dispatch_t: ops copied to the device (src/hive_dispatch.cu:583), the kernel,
+ * results copied back (src/hive_dispatch.cu:1096), done serially there. */
+int hive_insert_host(hive_table* t, const uint32_t* keys, const uint32_t* values, uint64_t n,
+                     uint8_t* status, void* stream);
+
+/* hive_find with keys, values and found in HOST memory: chunked upload, lookup and download
+ * overlapped as in hive_insert_host.  Either output may be NULL.  Same ordering rules. */
+int hive_find_host(hive_table* t, const uint32_t* keys, uint64_t n, uint32_t* values, uint8_t* found,
+                   void* stream);
+
 /* Bulk lookup: values[i] = value of keys[i] (0 if absent), found[i] = 0/1.  Either output may be
  * NULL.  Must not overlap on the GPU with a call that modifies the same table.
  * Replaces hive_lookup_kernel (include/hive_kernels.cuh:76-117), which discards the value. */
@@ -216,6 +233,26 @@ int hive_counters(hive_table* t, uint64_t* out, void* stream);
  * The reference has no counterpart (its lock spins are unbounded,
  * include/hive_hash_table_struct.cuh:101-117). */
 int hive_check(hive_table* t, void* stream);
+
+/* ---- launch tuning (hive_set_tuning / hive_get_tuning) ----------------------------------------
+ * Knobs of how a batch is run, never of what it computes: every setting gives the results of
+ * the one-at-a-time replay.  They replace the reference's compile-time launch constants
+ * (THREADS_PER_BLOCK / blocks-per-SM in src/hive_dispatch.cu) and are what an autotuner sets. */
+#define HIVE_TUNE_REGION_INSERT 0    /* 1: large inserts run in bucket-region order (a counting
+                                        sort first, statuses permuted back); 0 (default): in
+                                        submission order                                        */
+#define HIVE_TUNE_REGION_FIND 1      /* the same for hive_find; default 0                       */
+#define HIVE_TUNE_SUBBATCHES 2       /* sub-batches of a region-ordered insert, 1..8; 0 (default)
+                                        = chosen from the share of the capacity the batch adds   */
+#define HIVE_TUNE_SECOND_PASS_BLOCKS 3 /* resident blocks per SM of the second insert pass, 1..8;
+                                          default 4                                             */
+#define HIVE_NUM_TUNES 4
+
+/* Set knob `key` to `value`.  HIVE_ERR_INVALID_ARG for an unknown key or a value out of range. */
+int hive_set_tuning(hive_table* t, int32_t key, int64_t value);
+
+/* Read knob `key` into *value. */
+int hive_get_tuning(const hive_table* t, int32_t key, int64_t* value);
 
 /* Message for a status code; never NULL. */
 const char* hive_strerror(int status);

@@ -109,6 +109,89 @@ def test_bulk_sweep(cuda, policy, cap_log, lf):
         _assert_same_set(t, m)
 
 
+@pytest.mark.parametrize("policy", POLICIES)
+@pytest.mark.parametrize("subbatches", [0, 1, 3, 8])
+def test_region_ordered_batches(cuda, policy, subbatches):
+    """Region-ordered insert and find (counting sort by bucket region, statuses permuted back):
+    same per-op results and the same final key set as the replay, at 2^18 buckets (the smallest
+    table that takes the region path) and LF 0.95."""
+    cap = 1 << 21
+    n = int(0.95 * cap)
+    keys, absent, st = oracle.gen_keys(11, n, 1 << 16)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(cap, policy) as t:
+        t.set_tuning(region_insert=1, region_find=1, subbatches=subbatches)
+        assert t.tuning()["subbatches"] == subbatches
+        ins = _insert_and_check(t, m, keys, vals)
+        failed = int((ins == ST_FAIL).sum())
+        assert t.counters()["failed"] == failed
+        if subbatches in (0, 8):  # the automatic choice at this load is 8 sub-batches
+            assert failed == 0, failed
+        # re-insert a slice with new values: updates in region order
+        upd = keys[: n // 2][::-1].copy()
+        _insert_and_check(t, m, upd, oracle.values_for(upd) ^ np.uint32(0x5A5A5A5A))
+        look, _ = oracle.lookup_set(keys, absent, n // 2, 1 << 16, st)  # >= num_buckets lookups
+        _find_and_check(t, m, look)
+        _assert_same_set(t, m)
+        assert t.counters()["error_bits"] == 0
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_buffer_calls(cuda, pinned):
+    """hive_insert_host / hive_find_host: chunked uploads overlapped with the work.  Per-op results
+    equal the replay's and the key->value set equals the one hive_insert builds from the same
+    batch -- 2^23 slots at LF 0.9, two chunks."""
+    cap = 1 << 23
+    n = int(0.9 * cap)
+    keys, absent, st = oracle.gen_keys(5, n, 1 << 20)
+    vals = oracle.values_for(keys)
+    look, _ = oracle.lookup_set(keys, absent, 1 << 20, 1 << 20, st)
+    host = lambda a: torch.from_numpy(a.view(np.int32)).pin_memory() if pinned else a
+    m = oracle.ReplayMap()
+    with HiveHashTable(cap) as t, HiveHashTable(cap) as ref:
+        status = torch.empty(n, dtype=torch.uint8).pin_memory() if pinned else None
+        s = t.insert_host(host(keys), host(vals), status, sync=not pinned)
+        if pinned:
+            torch.cuda.current_stream().synchronize()
+        s = s.numpy()
+        exp = m.insert(keys, vals, apply_mask=(s != ST_FAIL).astype(np.uint8))
+        assert (s != ST_FAIL).all() and (exp == 1).all()
+        v, f = t.find_host(host(look))
+        ev, ef = m.find(look)
+        np.testing.assert_array_equal(f.numpy(), ef)
+        np.testing.assert_array_equal(v.numpy().view(np.uint32), ev)
+        _assert_same_set(t, m)
+        # the same batch through the device-buffer call: the same key->value set
+        ref.insert(keys, vals)
+        gk, gv = t.dump()
+        rk, rv = ref.dump()
+        np.testing.assert_array_equal(gk, rk)
+        np.testing.assert_array_equal(gv, rv)
+        # updates and an empty call through the host path
+        upd = np.ascontiguousarray(keys[::3])
+        s2 = t.insert_host(upd, upd).numpy()
+        np.testing.assert_array_equal(s2, np.full(upd.size, ST_UPDATED, np.uint8))
+        assert t.insert_host(np.empty(0, np.uint32), np.empty(0, np.uint32)).numel() == 0
+        v2, f2 = t.find_host(upd)
+        assert f2.numpy().all()
+        np.testing.assert_array_equal(v2.numpy().view(np.uint32), upd)
+        t.check()
+
+
+def test_tuning_bounds(cuda):
+    with HiveHashTable(1 << 12) as t:
+        assert t.tuning() == {"region_insert": 0, "region_find": 0, "subbatches": 0, "second_pass_blocks": 4}
+        for bad in ({"region_insert": 2}, {"subbatches": 9}, {"second_pass_blocks": 0}):
+            with pytest.raises(HiveError):
+                t.set_tuning(**bad)
+        t.set_tuning(second_pass_blocks=8)
+        keys, _, _ = oracle.gen_keys(3, 3000, 0)
+        m = oracle.ReplayMap()
+        _insert_and_check(t, m, keys, oracle.values_for(keys))
+        _assert_same_set(t, m)
+
+
 def test_reference_record_path(cuda):
     """16-byte Operation records, value = key + 1, uint64 0/1 results (the reference's kernel
     contract, include/hive_kernels.cuh:119-266)."""
