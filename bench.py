@@ -124,7 +124,9 @@ def random_bucket_ceiling(dev, table_bytes):
     """Throughput of the table's raw access patterns with nothing else in the kernel
     (hivehashtable_b200/csrc/hive_probe.cu): random 64 B bucket reads over a 4 GiB buffer, over a
     buffer the size of the table, over a 32 MiB L2-resident buffer; read + 8 B CAS; two dependent
-    reads.  GB/s counts 64 B per bucket read and 32 B per CAS'd sector."""
+    reads; two independent reads; one random 32 B sector; a CAS with and without a 32 B read before
+    it.  GB/s counts 64 B per bucket read, 32 B per sector read and 32 B per CAS'd sector; gops
+    counts threads (one op each)."""
     import ctypes
     import torch
     from hivehashtable_b200 import build as pbuild
@@ -139,7 +141,9 @@ def random_bucket_ceiling(dev, table_bytes):
     n = 1 << 26
     out = {}
     cases = [("read64_4GiB", 4 << 30, 0, 64), ("read64_table", table_bytes, 0, 64),
-             ("read64_cas_table", table_bytes, 1, 96), ("read64x2_table", table_bytes, 2, 128),
+             ("read32_table", table_bytes, 3, 32), ("read64_cas_table", table_bytes, 1, 96),
+             ("cas_only_table", table_bytes, 5, 32), ("read32_cas_table", table_bytes, 6, 64),
+             ("read64x2_table", table_bytes, 2, 128), ("read64x2_indep_table", table_bytes, 4, 128),
              ("read64_32MiB_l2", 32 << 20, 0, 64)]
     for name, size, mode, bpo in cases:
         buf = torch.zeros(size // 8, dtype=torch.int64, device=dev)
@@ -212,7 +216,7 @@ def workload_config(args, world, note=None):
                      f"{n:,} lookups ({args.present:.0%} present), {args.policy}",
          "capacity_slots": cap, "keys_per_gpu": n, "lookups_per_gpu": n, "present_fraction": args.present,
          "policy": args.policy, "seed": args.seed,
-         "l2": "inputs larger than L2 (table 512 MiB, each key array 241 MB); no flush",
+         "l2": f"inputs larger than L2 (table {cap * 8 >> 20} MiB, each key array {n * 4 / 1e6:.0f} MB); no flush",
          "parallelism": f"replicas: {world} independent table(s), one per GPU"}
     if note:
         d["note"] = note

@@ -10,6 +10,10 @@
 //   mode 1  read one random 64 B bucket, then CAS 8 B in it (value unchanged)
 //   mode 2  read two random 64 B buckets per thread (dependent: the second address comes from the
 //           first bucket's contents), the absent-key lookup pattern
+//   mode 3  read one random 32 B sector (half a bucket) per thread
+//   mode 4  read two random 64 B buckets per thread, both addresses known up front
+//   mode 5  CAS 8 B in a random bucket with no read before it (value unchanged)
+//   mode 6  read the random slot's 32 B sector, then CAS 8 B in it (value unchanged)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -47,7 +51,34 @@ __global__ void __launch_bounds__(256) k_probe(unsigned long long* buf, uint64_t
     const uint64_t b = mix64(i ^ seed) % nb;
     unsigned long long v[8];
     unsigned long long acc;
-    if (kMode == 1) {
+    if (kMode == 3) {
+        asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                     : "=l"(v[0]), "=l"(v[1]), "=l"(v[2]), "=l"(v[3])
+                     : "l"(buf + b * 8 + (i & 1) * 4));
+        acc = v[0] ^ v[1] ^ v[2] ^ v[3];
+    } else if (kMode == 4) {
+        unsigned long long w[8];
+        const uint64_t b2 = mix64(i ^ ~seed) % nb;
+        ld64(buf + b * 8, v);
+        ld64(buf + b2 * 8, w);
+        acc = v[0] ^ v[1] ^ v[2] ^ v[3] ^ v[4] ^ v[5] ^ v[6] ^ v[7] ^ w[0] ^ w[1] ^ w[2] ^ w[3] ^ w[4] ^ w[5] ^ w[6] ^
+              w[7];
+    } else if (kMode == 5) {
+        const int j = (int)(i & 7);
+        const unsigned long long g = (unsigned long long)(i * 0x9e3779b97f4a7c15ull);
+        acc = atomicCAS(buf + b * 8 + j, g, g);
+    } else if (kMode == 6) {
+        const int j = (int)(i & 7);
+        asm volatile("ld.relaxed.gpu.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                     : "=l"(v[0]), "=l"(v[1]), "=l"(v[2]), "=l"(v[3])
+                     : "l"(buf + b * 8 + (j & 4))
+                     : "memory");
+        unsigned long long cur = v[0];
+#pragma unroll
+        for (int q = 1; q < 4; ++q)
+            if (q == (j & 3)) cur = v[q];
+        acc = atomicCAS(buf + b * 8 + j, cur, cur);
+    } else if (kMode == 1) {
         ld64_relaxed(buf + b * 8, v);
         const int j = (int)(i & 7);
         unsigned long long cur = v[0];
@@ -74,7 +105,7 @@ extern "C" {
 // buf: device buffer of nb 64-byte buckets; n: buckets read (threads).  Returns a cudaError_t.
 __attribute__((visibility("default"))) int hive_probe_random_buckets(void* buf, uint64_t nb, uint64_t n, int mode,
                                                                       uint64_t seed, void* sink, void* stream) {
-    if (!buf || !nb || !sink || mode < 0 || mode > 2) return (int)cudaErrorInvalidValue;
+    if (!buf || !nb || !sink || mode < 0 || mode > 6) return (int)cudaErrorInvalidValue;
     if (!n) return 0;
     const unsigned grid = (unsigned)((n + 255) / 256);
     cudaStream_t s = (cudaStream_t)stream;
@@ -82,7 +113,11 @@ __attribute__((visibility("default"))) int hive_probe_random_buckets(void* buf, 
     auto* k = (unsigned long long*)sink;
     if (mode == 0) k_probe<0><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
     else if (mode == 1) k_probe<1><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
-    else k_probe<2><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else if (mode == 2) k_probe<2><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else if (mode == 3) k_probe<3><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else if (mode == 4) k_probe<4><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else if (mode == 5) k_probe<5><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else k_probe<6><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
     return (int)cudaGetLastError();
 }
 
