@@ -21,6 +21,19 @@
 //                                the reference probes victims' buckets one by one
 //   counters   u64[64 * 16]      slow-path event counters in 64 stripes of 16 words (summed by
 //                                the host) and the sticky error word (stripe 0, word 15)
+//   tags       u64[nb_cap]       byte j of tags[b] = an 8-bit fingerprint of the key in slot j of
+//                                bucket b (1..255), 0 when the slot is free.  64 MiB at 2^23
+//                                buckets against 512 MiB of slots: a lookup reads the tag words
+//                                and then only the 32 B sector whose fingerprint matches, and an
+//                                absent key usually reads no slot at all.  Random 32 B sector
+//                                reads run at about 1.7x the rate of 64 B bucket reads on B200.
+//                                Invariant: an occupied slot's byte holds its key's fingerprint.
+//                                Small batches keep it per op (the claimer publishes the byte
+//                                after its claim CAS); a bulk insert skips the upkeep and
+//                                rebuilds every tag word from the slots afterwards (k_retag).  A
+//                                free slot's byte is 0 as long as no delete or resize ran since
+//                                the last clear; afterwards it may hold a stale fingerprint,
+//                                which costs a read but never hides a key.
 //
 // A slot holds (value << 32) | key (include/hive_hash_table_struct.cuh:297-311); key 0 is the
 // empty sentinel, so an all-zero slot is free (include/utils.h:39-47).  There is no freeMask
@@ -59,7 +72,9 @@ enum {
 };
 enum : unsigned long long { kErrLockTimeout = 1ull, kErrRetryOut = 2ull };
 
-constexpr uint32_t kFlagHoles = 1u;  // deletes or a resize ran since the last clear
+constexpr uint32_t kFlagHoles = 1u;     // deletes or a resize ran since the last clear
+constexpr uint32_t kFlagUntagged = 2u;  // set on the launch's copy only: this launch leaves the
+                                        // tag words to a rebuild after it (k_retag)
 
 // The device view of a table, passed to every kernel by value.
 //
@@ -74,6 +89,7 @@ struct Table {
     uint32_t* locks;
     uint32_t* full_bits;
     u64* counters;
+    u64* tags;
     u64 m_lo;  // fastmod magic for n_lo
     u64 m_hi;  // fastmod magic for 2 * n_lo
     uint32_t n_lo;
@@ -310,34 +326,172 @@ __device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
 __device__ __forceinline__ void unlock_bucket(const Table& t, uint32_t b) { atomicExch(t.locks + b, 0u); }
 
 // ---------------------------------------------------------------------------------------------
+// Slot tags (see the layout above)
+// ---------------------------------------------------------------------------------------------
+
+// The key's 8-bit fingerprint, never 0; a mixer of its own, unrelated to the bucket hashes.
+__host__ __device__ __forceinline__ uint32_t tag_of(uint32_t k) {
+    const uint32_t f = fmix32(k ^ 0x2545F491u) >> 24;
+    return f ? f : 1u;
+}
+
+// 0xFF/0x00 per byte -> one bit per byte (the four multiplied bits land on distinct positions).
+__device__ __forceinline__ uint32_t byte_bits(uint32_t m) { return ((m & 0x01010101u) * 0x01020408u) >> 24; }
+
+// Bit j set: byte j of the tag word equals f (f = 0: the free slots).
+__device__ __forceinline__ uint32_t tag_match(u64 T, uint32_t f) {
+    const uint32_t rep = f * 0x01010101u;
+    return byte_bits(__vcmpeq4((uint32_t)T, rep)) | (byte_bits(__vcmpeq4((uint32_t)(T >> 32), rep)) << 4);
+}
+
+__device__ __forceinline__ u64 ld_relaxed_u64(const u64* p) {
+    u64 v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ u64 load_tags(const Table& t, uint32_t b) { return ld_relaxed_u64(t.tags + b); }
+__device__ __forceinline__ u64 load_tags_ro(const Table& t, uint32_t b) {
+    u64 v;
+    asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(t.tags + b));
+    return v;
+}
+
+// The claim of a free slot on a table without holes: the byte is 0 and only the winner of the
+// slot's claim CAS writes it, so an OR is exact; fire-and-forget.
+__device__ __forceinline__ void tag_publish(const Table& t, uint32_t b, int j, uint32_t f) {
+    asm volatile("red.relaxed.gpu.global.or.b64 [%0], %1;" ::"l"(t.tags + b), "l"((u64)f << (8 * j)) : "memory");
+}
+
+// Byte j := f, other bytes unchanged (a claim on a table with holes, or an eviction's overwrite).
+// The word CAS completes before the caller's next access, so a reader that finds the slot's new
+// contents through a later step also finds its fingerprint.  tag_set and tag_clear do nothing in
+// a launch without tag upkeep (kFlagUntagged).
+__device__ __forceinline__ void tag_set(const Table& t, uint32_t b, int j, uint32_t f) {
+    if (t.flags & kFlagUntagged) return;
+    u64* w = t.tags + b;
+    const u64 mask = 0xFFull << (8 * j), val = (u64)f << (8 * j);
+    u64 old = ld_relaxed_u64(w);
+    for (int r = 0; r < kRetryLimit; ++r) {
+        const u64 nw = (old & ~mask) | val;
+        if (nw == old) return;
+        const u64 obs = atomicCAS(w, old, nw);
+        if (obs == old) return;
+        old = obs;
+    }
+    count(t, kCtrRetryOut);
+    raise_error(t, kErrRetryOut);
+}
+
+// Byte j := 0 after slot j was freed, unless the slot has been claimed again meanwhile (then its
+// claimer writes the byte).  A claimer's tag_set that lands between this check and the CAS
+// changes the word, so the CAS fails and the check runs again.
+__device__ __forceinline__ void tag_clear(const Table& t, uint32_t b, int j) {
+    if (t.flags & kFlagUntagged) return;
+    u64* w = t.tags + b;
+    const u64 mask = 0xFFull << (8 * j);
+    const u64* slot = t.slots + (size_t)b * kSlots + j;
+    u64 old = ld_relaxed_u64(w);
+    for (int r = 0; r < kRetryLimit; ++r) {
+        if (!(old & mask)) return;
+        if (ld_relaxed_u64(slot) != 0ull) return;
+        const u64 obs = atomicCAS(w, old, old & ~mask);
+        if (obs == old) return;
+        old = obs;
+    }
+    count(t, kCtrRetryOut);
+    raise_error(t, kErrRetryOut);
+}
+
+// The tag word of a bucket's contents (the rebuild and the resize kernels, which own the buckets
+// they rewrite).
+__device__ __forceinline__ u64 tag_word(const u64 (&s)[kSlots]) {
+    u64 w = 0;
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j)
+        if (s[j]) w |= (u64)tag_of(key_of(s[j])) << (8 * j);
+    return w;
+}
+
+// One 32 B sector (slots 4s .. 4s + 3) of bucket p.
+struct Sector {
+    u64 s[4];
+};
+__device__ __forceinline__ void load_sector_ro(const u64* p, Sector& S) {
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(S.s[0]), "=l"(S.s[1]), "=l"(S.s[2]), "=l"(S.s[3])
+                 : "l"(p));
+}
+__device__ __forceinline__ void load_sector(const u64* p, Sector& S) {
+    asm volatile("ld.relaxed.gpu.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(S.s[0]), "=l"(S.s[1]), "=l"(S.s[2]), "=l"(S.s[3])
+                 : "l"(p)
+                 : "memory");
+}
+__device__ __forceinline__ uint32_t sector_match(const Sector& S, uint32_t k) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) m |= (uint32_t)(key_of(S.s[j]) == k) << j;
+    return m;
+}
+__device__ __forceinline__ u64 sector_at(const Sector& S, int j) {
+    u64 r = S.s[0];
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+        if (q == j) r = S.s[q];
+    return r;
+}
+
+// Find k in bucket b using its tag word T: reads only the sectors holding a matching fingerprint.
+template <bool kReadOnly>
+__device__ __forceinline__ bool find_tagged(const Table& t, uint32_t b, u64 T, uint32_t k, uint32_t f, uint32_t* v) {
+    uint32_t m = tag_match(T, f);
+    while (m) {
+        const int sec = (__ffs(m) - 1) >> 2;
+        m &= ~(0xFu << (4 * sec));
+        Sector S;
+        if (kReadOnly) load_sector_ro(t.slots + (size_t)b * kSlots + 4 * sec, S);
+        else load_sector(t.slots + (size_t)b * kSlots + 4 * sec, S);
+        const uint32_t hit = sector_match(S, k);
+        if (hit) {
+            *v = val_of(sector_at(S, __ffs(hit) - 1));
+            return true;
+        }
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Lookup: H0, H1, then the canonical stash gated by its flag
 // (include/hive_hash_lookup.cuh:126-155)
 // ---------------------------------------------------------------------------------------------
 
+// The slots are read only where a fingerprint matches; the stash has no tags and is read whole
+// when its flag is set.  Read-only kernels (nothing changes during the launch) read both tag
+// words up front, two independent L2 reads.  Otherwise H1's tags are read only after H0 missed:
+// an eviction writes the victim (and its fingerprint) to H1 before removing it from H0, so
+// reading H0 then H1 in that order always finds it.
 template <int P, bool kReadOnly>
 __device__ __forceinline__ bool find_one(const Table& t, uint32_t k, uint32_t* v) {
     if (k == 0) return false;
+    const uint32_t f = tag_of(k);
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
-    Bucket B;
-    if (kReadOnly) load_bucket_ro(t.slots + (size_t)b0 * kSlots, B);
-    else load_bucket(t.slots + (size_t)b0 * kSlots, B);
-    uint32_t m = match_mask(B, k);
-    if (!m) {
-        const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
-        if (b1 != b0) {
-            if (kReadOnly) load_bucket_ro(t.slots + (size_t)b1 * kSlots, B);
-            else load_bucket(t.slots + (size_t)b1 * kSlots, B);
-            m = match_mask(B, k);
+    const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
+    const u64 T0 = kReadOnly ? load_tags_ro(t, b0) : load_tags(t, b0);
+    u64 T1 = kReadOnly ? load_tags_ro(t, b1) : 0ull;
+    if (find_tagged<kReadOnly>(t, b0, T0, k, f, v)) return true;
+    if (!kReadOnly) T1 = load_tags(t, b1);
+    if (b1 != b0 && find_tagged<kReadOnly>(t, b1, T1, k, f, v)) return true;
+    if (kReadOnly ? stash_flag_ro(t, b0) : stash_flag(t, b0)) {
+        Bucket B;
+        if (kReadOnly) load_bucket_ro(t.stash + (size_t)b0 * kSlots, B);
+        else load_bucket(t.stash + (size_t)b0 * kSlots, B);
+        const uint32_t m = match_mask(B, k);
+        if (m) {
+            *v = val_of(slot_at(B, __ffs(m) - 1));
+            return true;
         }
-        if (!m && (kReadOnly ? stash_flag_ro(t, b0) : stash_flag(t, b0))) {
-            if (kReadOnly) load_bucket_ro(t.stash + (size_t)b0 * kSlots, B);
-            else load_bucket(t.stash + (size_t)b0 * kSlots, B);
-            m = match_mask(B, k);
-        }
-        if (!m) return false;
     }
-    *v = val_of(slot_at(B, __ffs(m) - 1));
-    return true;
+    return false;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -373,8 +527,9 @@ __device__ __forceinline__ int increment_in(u64* p, uint32_t k, uint32_t* nv) {
 // same key can claim different slots.  Keep the lower-indexed copy; whichever of the two racing
 // inserts sees the other removes the higher one (a CAS from the exact value, so at most one
 // removal happens and nothing else is ever removed).  Returns true if this op's own copy was
-// the one removed.
-__device__ __forceinline__ bool resolve_duplicate(const Table& t, u64* p, uint32_t k, int j, u64 kv) {
+// the one removed.  b is the bucket's index (the removed copy's fingerprint is cleared).
+__device__ __forceinline__ bool resolve_duplicate(const Table& t, uint32_t b, uint32_t k, int j, u64 kv) {
+    u64* p = t.slots + (size_t)b * kSlots;
     __threadfence();
     Bucket B;
     load_bucket(p, B);
@@ -383,13 +538,17 @@ __device__ __forceinline__ bool resolve_duplicate(const Table& t, u64* p, uint32
     int o = __ffs(m) - 1;
     if (o < j) {
         if (cas64(p + j, kv, 0ull) == kv) {
+            tag_clear(t, b, j);
             count(t, kCtrDupFixed);
             return true;
         }
         return false;
     }
     u64 theirs = slot_at(B, o);
-    if (cas64(p + o, theirs, 0ull) == theirs) count(t, kCtrDupFixed);
+    if (cas64(p + o, theirs, 0ull) == theirs) {
+        tag_clear(t, b, o);
+        count(t, kCtrDupFixed);
+    }
     return false;
 }
 
@@ -431,7 +590,11 @@ __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket&
         alts[j] = b0;
         if (j >= limit) continue;
         const u64 vkv = B0.s[j];
-        if (vkv == 0ull) return cas64(B0p + j, 0ull, kv) == 0ull ? kEvPlaced : kEvRetry;
+        if (vkv == 0ull) {
+            if (cas64(B0p + j, 0ull, kv) != 0ull) return kEvRetry;
+            tag_set(t, b0, j, tag_of(key_of(kv)));
+            return kEvPlaced;
+        }
         const uint32_t vk = key_of(vkv);
         if (bucket_addr(t, Policy<P>::h0(vk)) != b0) continue;  // victim lives in its H1
         const uint32_t alt = bucket_addr(t, Policy<P>::h1(vk));
@@ -466,17 +629,26 @@ __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket&
         const int d = __ffs(e) - 1;
         if (cas64(Ap + d, 0ull, vkv) != 0ull) continue;  // lost the free slot; next victim
         if (__popc(e) == 1) mark_full(t, alt);
+        // The copy's fingerprint is in place before H0's slot changes (tag_set completes).
+        tag_set(t, alt, d, tag_of(vk));
         // The victim is now visible in both H0 slot j and H1 slot d.
+        const uint32_t f = tag_of(key_of(kv));
         for (int r = 0; r < kRetryLimit; ++r) {
             u64 obs = cas64(B0p + j, vkv, kv);
             if (obs == vkv) {
+                tag_set(t, b0, j, f);
                 count(t, kCtrEvictions);
                 return kEvPlaced;
             }
             if (obs == 0ull) {
                 // Victim deleted meanwhile: drop the copy unless it changed, take the free slot.
-                if (cas64(Ap + d, vkv, 0ull) == vkv) mark_not_full(t, alt);
-                return cas64(B0p + j, 0ull, kv) == 0ull ? kEvPlaced : kEvRetry;
+                if (cas64(Ap + d, vkv, 0ull) == vkv) {
+                    tag_clear(t, alt, d);
+                    mark_not_full(t, alt);
+                }
+                if (cas64(B0p + j, 0ull, kv) != 0ull) return kEvRetry;
+                tag_set(t, b0, j, f);
+                return kEvPlaced;
             }
             if (key_of(obs) == vk) {
                 // Victim updated meanwhile: carry the new value to the copy, then retry.
@@ -484,7 +656,10 @@ __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket&
                 vkv = obs;
                 continue;
             }
-            if (cas64(Ap + d, vkv, 0ull) == vkv) mark_not_full(t, alt);
+            if (cas64(Ap + d, vkv, 0ull) == vkv) {
+                tag_clear(t, alt, d);
+                mark_not_full(t, alt);
+            }
             return kEvRetry;
         }
         count(t, kCtrRetryOut);
@@ -528,8 +703,9 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         if (e) {
             int j = __ffs(e) - 1;
             if (cas64(B0p + j, 0ull, kv) == 0ull) {
+                tag_set(t, b0, j, tag_of(k));
                 if (__popc(e) == 1) mark_full(t, b0);
-                if (holes && resolve_duplicate(t, B0p, k, j, kv)) return kStUpdated;
+                if (holes && resolve_duplicate(t, b0, k, j, kv)) return kStUpdated;
                 return kStInserted;
             }
             continue;
@@ -538,8 +714,9 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         if (e) {
             int j = __ffs(e) - 1;
             if (cas64(B1p + j, 0ull, kv) == 0ull) {
+                tag_set(t, b1, j, tag_of(k));
                 if (__popc(e) == 1) mark_full(t, b1);
-                if (holes && resolve_duplicate(t, B1p, k, j, kv)) return kStUpdated;
+                if (holes && resolve_duplicate(t, b1, k, j, kv)) return kStUpdated;
                 return kStInserted;
             }
             continue;
@@ -571,35 +748,103 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
     return kStError;
 }
 
-// Without holes: update k in bucket p or claim p's lowest free slot.  Returns kStUpdated /
-// kStInserted, or 0 when p is full (or its retry budget ran out: the locked path finishes).
-__device__ __forceinline__ uint8_t claim_or_update(const Table& t, uint32_t b, uint32_t k, u64 kv) {
+// Update the value of k in slot j of bucket p, whose current contents are `cur` (key k).
+// Returns kStUpdated, or 0 if the retry budget ran out (the locked path finishes the op).
+__device__ __forceinline__ uint8_t update_slot(u64* p, int j, u64 cur, u64 kv) {
+    for (int r = 0; r < kRetryLimit; ++r) {
+        const u64 obs = cas64(p + j, cur, kv);
+        if (obs == cur) return kStUpdated;
+        cur = obs;  // a racing update of the same key; slots never change keys without holes
+    }
+    return 0;
+}
+
+// Without holes and without tag upkeep (a bulk insert whose tag words are rebuilt after it):
+// update k in bucket b or claim b's lowest free slot from one 64 B read of the bucket.
+// Returns kStUpdated / kStInserted, or 0 when b is full or a budget ran out.
+__device__ __forceinline__ uint8_t claim_or_update_untagged(const Table& t, uint32_t b, uint32_t k, u64 kv) {
     u64* p = t.slots + (size_t)b * kSlots;
     for (int r = 0; r < kRetryLimit; ++r) {
         Bucket B;
         load_bucket(p, B);
-        uint32_t m = match_mask(B, k);
+        const uint32_t m = match_mask(B, k);
         if (m) {
-            int j = __ffs(m) - 1;
-            u64 old = slot_at(B, j);
-            if (cas64(p + j, old, kv) == old) return kStUpdated;
-            continue;
+            const int j = __ffs(m) - 1;
+            return update_slot(p, j, slot_at(B, j), kv);
         }
-        uint32_t e = empty_mask(B);
+        const uint32_t e = empty_mask(B);
         if (!e) return 0;
-        if (cas64(p + (__ffs(e) - 1), 0ull, kv) == 0ull) {
+        const int j = __ffs(e) - 1;
+        const u64 obs = cas64(p + j, 0ull, kv);
+        if (obs == 0ull) {
             if (__popc(e) == 1) mark_full(t, b);
             return kStInserted;
+        }
+        if (key_of(obs) == k) return update_slot(p, j, obs, kv);
+    }
+    return 0;
+}
+
+// Without holes, with tag upkeep: update k in bucket b or claim b's lowest free slot, guided by
+// b's tag word.  Without holes the free slots by the tag word are a superset of the truly free
+// ones (a claim publishes its fingerprint after its CAS), so trying them in ascending order
+// reaches the lowest free slot, and two inserts of one key race for the same slot: one CAS wins
+// and the other sees the key and updates it.  A key already in b has its fingerprint published
+// unless its claim races with this op, which the sector snapshot or the CAS then shows.  Only the
+// sector holding a candidate slot is read, before its CAS: a CAS that misses L2 runs far slower
+// than a 32 B read followed by a CAS that hits.  Returns as claim_or_update_untagged.
+template <bool kTagged = true>
+__device__ __forceinline__ uint8_t claim_or_update(const Table& t, uint32_t b, uint32_t k, u64 kv) {
+    if (!kTagged) return claim_or_update_untagged(t, b, k, kv);
+    u64* p = t.slots + (size_t)b * kSlots;
+    const uint32_t f = tag_of(k);
+    const u64 T = load_tags(t, b);
+    uint32_t m = tag_match(T, f);
+    while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1;
+        const u64 cur = ld_relaxed_u64(p + j);
+        if (key_of(cur) == k) return update_slot(p, j, cur, kv);
+    }
+    uint32_t e = tag_match(T, 0u);
+    while (e) {
+        const int sec = (__ffs(e) - 1) >> 2;
+        uint32_t es = (e >> (4 * sec)) & 0xFu;
+        e &= ~(0xFu << (4 * sec));
+        u64* sp = p + 4 * sec;
+        Sector S;
+        load_sector(sp, S);
+        const uint32_t hit = sector_match(S, k);
+        if (hit) {
+            const int q = __ffs(hit) - 1;
+            return update_slot(sp, q, sector_at(S, q), kv);
+        }
+        while (es) {
+            const int q = __ffs(es) - 1;
+            es &= es - 1;
+            if (sector_at(S, q) != 0ull) continue;  // taken by a claim still publishing its tag
+            const u64 obs = cas64(sp + q, 0ull, kv);
+            if (obs == 0ull) {
+                tag_publish(t, b, 4 * sec + q, f);
+                if (!e && !es) mark_full(t, b);  // every other slot carries a fingerprint
+                return kStInserted;
+            }
+            if (key_of(obs) == k) return update_slot(sp, q, obs, kv);
         }
     }
     return 0;
 }
 
 // Which insert protocol a kernel compiles: chosen from the table's flags at run time, or fixed
-// by the host (which knows the flags) so the kernel carries only the code it needs.
-// kModeMonoPrimary is kModeMono whose deferring first pass claims in H0 only (region-ordered
-// batches, see insert_lockfree).
-enum Mode { kModeRuntime = 0, kModeMono = 1, kModeHoles = 2, kModeMonoPrimary = 3 };
+// by the host (which knows the flags) so the kernel carries only the code it needs.  The base
+// (low two bits) says whether the table may have holes; two flag bits refine it:
+//   kModePrimary   a deferring first pass claims in H0 only (region-ordered batches, see
+//                  insert_lockfree)
+//   kModeUntagged  no tag upkeep: a bulk insert whose tag words are rebuilt after it; the
+//                  launch's Table copy carries kFlagUntagged for the code chosen at run time
+enum Mode { kModeRuntime = 0, kModeMono = 1, kModeHoles = 2, kModePrimary = 4, kModeUntagged = 8 };
+__host__ __device__ constexpr int mode_base(int m) { return m & 3; }
+__device__ __forceinline__ bool tagged(const Table& t) { return !(t.flags & kFlagUntagged); }
 
 // Lock-free stages A and B.  Returns the op's final status, or 0 when the op must go on: to the
 // locked path (stages C/D) when H0 and H1 are both full, or -- with kPrimaryOnly, the first pass
@@ -613,11 +858,12 @@ template <int P, int kMode = kModeRuntime, bool kPrimaryOnly = false>
 __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
     u64* B0p = t.slots + (size_t)b0 * kSlots;
     u64* B1p = t.slots + (size_t)b1 * kSlots;
-    const bool holes = kMode == kModeHoles || (kMode == kModeRuntime && (t.flags & kFlagHoles));
+    constexpr bool kTagged = !(kMode & kModeUntagged);
+    const bool holes = mode_base(kMode) == kModeHoles || (mode_base(kMode) == kModeRuntime && (t.flags & kFlagHoles));
     if (!holes) {
-        uint8_t st = claim_or_update(t, b0, k, kv);
+        uint8_t st = claim_or_update<kTagged>(t, b0, k, kv);
         if (st || b1 == b0 || kPrimaryOnly) return st;
-        return claim_or_update(t, b1, k, kv);
+        return claim_or_update<kTagged>(t, b1, k, kv);
     }
     // With holes a key may sit in H1 or the stash while H0 has room: scan all three first.
     u64* Sp = t.stash + (size_t)b0 * kSlots;
@@ -655,8 +901,9 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
         if (!e) return 0;
         int j = __ffs(e) - 1;
         if (cas64(Cp + j, 0ull, kv) == 0ull) {
+            if (kTagged) tag_set(t, cb, j, tag_of(k));
             if (__popc(e) == 1) mark_full(t, cb);
-            return resolve_duplicate(t, Cp, k, j, kv) ? kStUpdated : kStInserted;
+            return resolve_duplicate(t, cb, k, j, kv) ? kStUpdated : kStInserted;
         }
     }
     return 0;
@@ -680,7 +927,7 @@ __device__ __forceinline__ uint8_t insert_one(const Table& t, uint32_t k, uint32
     const u64 kv = pack(k, v);
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
     const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
-    uint8_t st = insert_lockfree<P, kMode, kDefer && kMode == kModeMonoPrimary>(t, k, kv, b0, b1);
+    uint8_t st = insert_lockfree<P, kMode, kDefer && (kMode & kModePrimary) != 0>(t, k, kv, b0, b1);
     if (st) return st;
     if (kDefer) return kStDefer;
     return insert_locked_path<P>(t, k, kv, b0, b1);
@@ -696,7 +943,7 @@ __device__ __forceinline__ uint8_t insert_deferred_one(const Table& t, uint32_t 
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
     const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
     if (b1 != b0) {
-        const uint8_t st = claim_or_update(t, b1, k, kv);
+        const uint8_t st = tagged(t) ? claim_or_update<true>(t, b1, k, kv) : claim_or_update<false>(t, b1, k, kv);
         if (st) return st;
     }
     return insert_locked_path<P>(t, k, kv, b0, b1);
@@ -708,7 +955,9 @@ __device__ __forceinline__ uint8_t insert_deferred_one(const Table& t, uint32_t 
 // ---------------------------------------------------------------------------------------------
 // Removes every copy of k from bucket p.  is_slots: p is table bucket b (not a stash), whose
 // full hint is cleared after a removal.
+// A table bucket whose tag word holds no matching fingerprint is not read.
 __device__ __forceinline__ bool erase_in(const Table& t, u64* p, uint32_t k, bool is_slots, uint32_t b) {
+    if (is_slots && !tag_match(load_tags(t, b), tag_of(k))) return false;
     bool removed = false;
     for (int r = 0; r < kRetryLimit; ++r) {
         Bucket B;
@@ -720,7 +969,10 @@ __device__ __forceinline__ bool erase_in(const Table& t, u64* p, uint32_t k, boo
         }
         int j = __ffs(m) - 1;
         u64 old = slot_at(B, j);
-        if (cas64(p + j, old, 0ull) == old) removed = true;
+        if (cas64(p + j, old, 0ull) == old) {
+            removed = true;
+            if (is_slots) tag_clear(t, b, j);
+        }
     }
     if (removed && is_slots) mark_not_full(t, b);
     count(t, kCtrRetryOut);

@@ -69,13 +69,13 @@ struct hive_table {
     uint32_t level = 0;
     void* block = nullptr;   // single allocation holding every array
     size_t block_bytes = 0;
-    u64* scratch = nullptr;  // device words: [0] size/dump count, [1] deferred-op count
+    u64* scratch = nullptr;  // device words: [0] size/dump count, [1] deferred-op count, [2, 6) verify
     uint32_t* defer_q = nullptr;  // deferred-op queue (one index per op of the largest batch)
     uint64_t defer_cap = 0;
     void* rbuf = nullptr;         // region-ordering buffers (13 bytes per op of the largest batch)
     uint64_t rcap = 0;
     int num_sms = 148;
-    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4};  // HIVE_TUNE_* knobs
+    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1};  // HIVE_TUNE_* knobs
     // host-buffer pipeline (hive_insert_host / hive_find_host): copy streams, events and device
     // staging arrays (insert keys, values, statuses; find keys, values, flags: 18 bytes per op)
     cudaStream_t pipe_h2d = nullptr, pipe_d2h = nullptr;
@@ -102,7 +102,7 @@ constexpr size_t kCounterBytes = (size_t)hive::kCounterStripes * hive::kCounterS
 static_assert(hive::kCounterStride >= HIVE_NUM_COUNTERS, "a counter stripe holds every counter");
 
 struct Carve {
-    size_t slots, stash, sbits, lbits, fbits, ctr, scratch, total;
+    size_t slots, stash, sbits, lbits, fbits, ctr, tags, scratch, total;
 };
 Carve carve(uint64_t nb_cap) {
     Carve c;
@@ -113,8 +113,9 @@ Carve carve(uint64_t nb_cap) {
     c.lbits = align256(c.sbits + words * 4);
     c.fbits = align256(c.lbits + (size_t)nb_cap * 4);
     c.ctr = align256(c.fbits + words * 4);
-    c.scratch = align256(c.ctr + kCounterBytes);
-    c.total = align256(c.scratch + 16);
+    c.tags = align256(c.ctr + kCounterBytes);
+    c.scratch = align256(c.tags + (size_t)nb_cap * 8);
+    c.total = align256(c.scratch + 48);  // 6 scratch words
     return c;
 }
 
@@ -130,6 +131,7 @@ void bind_arrays(hive_table* h, void* block, uint64_t nb_cap) {
     h->t.locks = (uint32_t*)(base + c.lbits);
     h->t.full_bits = (uint32_t*)(base + c.fbits);
     h->t.counters = (u64*)(base + c.ctr);
+    h->t.tags = (u64*)(base + c.tags);
     h->scratch = (u64*)(base + c.scratch);
 }
 
@@ -169,7 +171,7 @@ __device__ __forceinline__ void defer_push(const Defer& d, bool deferred, uint64
 // over ops [lo, hi) of the batch; deferred ops are queued by their index in the batch, so the
 // first passes of several chunks of one batch feed one second pass.
 template <int P, bool kDefer, int kMode>
-__global__ void __launch_bounds__(kBlock, (kDefer && (kMode == hive::kModeMono || kMode == hive::kModeMonoPrimary)) ? 8 : 1)
+__global__ void __launch_bounds__(kBlock, (kDefer && hive::mode_base(kMode) == hive::kModeMono) ? 8 : 1)
     k_insert(hive::Table t, const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, uint64_t lo,
              uint64_t hi, uint8_t* __restrict__ status, Defer d) {
     const uint64_t i = lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x;
@@ -570,6 +572,51 @@ __global__ void k_dump(hive::Table t, uint64_t nb, u64* __restrict__ kv, uint64_
     }
 }
 
+// Structural check of buckets [0, nb) and their stashes; out[HIVE_VERIFY_*] counts violations:
+// a slot whose tag byte is not its key's fingerprint, a key in neither of its buckets (a stash
+// entry not under its canonical bucket), a key twice in one bucket, and -- only when the table has
+// no holes (strict) -- a free slot with a nonzero tag byte.
+template <int P>
+__global__ void k_verify(hive::Table t, uint64_t nb, bool strict, u64* out) {
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    hive::Bucket B;
+    hive::load_bucket_ro(t.slots + b * hive::kSlots, B);
+    const u64 T = t.tags[b];
+    u64 bad[HIVE_VERIFY_COUNT] = {0, 0, 0, 0};
+    for (int j = 0; j < hive::kSlots; ++j) {
+        const u64 kv = B.s[j];
+        const uint32_t byte = (uint32_t)(T >> (8 * j)) & 0xFFu;
+        if (!kv) {
+            bad[HIVE_VERIFY_STALE_TAG] += strict && byte != 0;
+            continue;
+        }
+        const uint32_t k = hive::key_of(kv);
+        bad[HIVE_VERIFY_TAG_MISMATCH] += byte != hive::tag_of(k);
+        bad[HIVE_VERIFY_MISPLACED] +=
+            hive::bucket_addr(t, hive::Policy<P>::h0(k)) != b && hive::bucket_addr(t, hive::Policy<P>::h1(k)) != b;
+        for (int q = 0; q < j; ++q) bad[HIVE_VERIFY_DUPLICATE] += hive::key_of(B.s[q]) == k;
+    }
+    if ((t.stash_bits[b >> 5] >> (b & 31)) & 1u) {
+        hive::load_bucket_ro(t.stash + b * hive::kSlots, B);
+        for (int j = 0; j < hive::kSlots; ++j)
+            if (B.s[j])
+                bad[HIVE_VERIFY_MISPLACED] += hive::bucket_addr(t, hive::Policy<P>::h0(hive::key_of(B.s[j]))) != b;
+    }
+    for (int c = 0; c < HIVE_VERIFY_COUNT; ++c)
+        if (bad[c]) atomicAdd(out + c, bad[c]);
+}
+
+// Tag words of buckets [0, nb) recomputed from their slots (after an untagged bulk insert): one
+// coalesced pass, 64 B read and 8 B written per bucket.
+__global__ void __launch_bounds__(kBlock) k_retag(hive::Table t, uint64_t nb) {
+    const uint64_t b = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (b >= nb) return;
+    hive::Bucket B;
+    hive::load_bucket_ro(t.slots + b * hive::kSlots, B);
+    t.tags[b] = hive::tag_word(B.s);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Resize: linear hashing.  Split moves the keys of buckets [s, s + cnt) that now address
 // b + n_lo; merge folds buckets [s - cnt + n_lo, s + n_lo) back into [s - cnt, s).  Both run
@@ -599,19 +646,23 @@ __global__ void k_split(hive::Table told, hive::Table tnew, uint32_t s, uint32_t
     u64* dst = told.slots + (size_t)nbk * hive::kSlots;
     hive::Bucket B;
     hive::load_bucket(src, B);
-    int nd = 0;
-    u64 keep[hive::kSlots];
-    int nk = 0;
+    // new contents of b (keep) and of b + n_lo (moved), written with their tag words at the end
+    u64 keep[hive::kSlots], moved[hive::kSlots];
+    int nk = 0, nd = 0;
+#pragma unroll
+    for (int j = 0; j < hive::kSlots; ++j) {
+        keep[j] = 0ull;
+        moved[j] = 0ull;
+    }
 #pragma unroll
     for (int j = 0; j < hive::kSlots; ++j) {
         const u64 kv = B.s[j];
         if (!kv) continue;
         bool via0;
         const uint32_t h = resident_hash<P>(told, hive::key_of(kv), b, &via0);
-        if (hive::bucket_addr(tnew, h) == nbk) dst[nd++] = kv;
+        if (hive::bucket_addr(tnew, h) == nbk) moved[nd++] = kv;
         else keep[nk++] = kv;
     }
-    for (int j = 0; j < hive::kSlots; ++j) src[j] = j < nk ? keep[j] : 0ull;
     // Stash entries of canonical bucket b: re-place them by their new canonical bucket, into a
     // free slot when there is one, else into that bucket's stash.
     if ((told.stash_bits[b >> 5] >> (b & 31)) & 1u) {
@@ -626,9 +677,9 @@ __global__ void k_split(hive::Table told, hive::Table tnew, uint32_t s, uint32_t
             if (!kv) continue;
             const uint32_t c = hive::bucket_addr(tnew, hive::Policy<P>::h0(hive::key_of(kv)));
             if (c == b && nk < hive::kSlots) {
-                src[nk++] = kv;
+                keep[nk++] = kv;
             } else if (c == nbk && nd < hive::kSlots) {
-                dst[nd++] = kv;
+                moved[nd++] = kv;
             } else if (c == b) {
                 ks[keep_s++] = kv;
             } else {
@@ -639,6 +690,13 @@ __global__ void k_split(hive::Table told, hive::Table tnew, uint32_t s, uint32_t
         if (!keep_s) atomicAnd(told.stash_bits + (b >> 5), ~(1u << (b & 31)));
         if (moved_s) atomicOr(told.stash_bits + (nbk >> 5), 1u << (nbk & 31));
     }
+#pragma unroll
+    for (int j = 0; j < hive::kSlots; ++j) {
+        src[j] = keep[j];
+        dst[j] = moved[j];
+    }
+    told.tags[b] = hive::tag_word(keep);
+    told.tags[nbk] = hive::tag_word(moved);
     if (nk == hive::kSlots) hive::mark_full(told, b);
     else hive::mark_not_full(told, b);
     if (nd == hive::kSlots) hive::mark_full(told, nbk);
@@ -675,6 +733,8 @@ __global__ void k_merge(hive::Table told, hive::Table tnew, uint32_t lo, uint32_
     hive::Bucket D;
     hive::load_bucket(tnew.slots + (size_t)b * hive::kSlots, D);
     if (!hive::empty_mask(D)) hive::mark_full(told, b);
+    told.tags[b] = hive::tag_word(D.s);
+    told.tags[src_b] = 0ull;
 }
 
 // Re-insert overflow entries produced by k_merge through the normal insert protocol.
@@ -707,6 +767,7 @@ int reset(hive_table* h, cudaStream_t s) {
     HIVE_CUDA(cudaMemsetAsync(h->t.locks, 0, (size_t)nb * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.full_bits, 0, (size_t)words * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.counters, 0, kCounterBytes, s));
+    HIVE_CUDA(cudaMemsetAsync(h->t.tags, 0, (size_t)nb * 8, s));
     return HIVE_OK;
 }
 
@@ -833,6 +894,8 @@ int grow_capacity(hive_table* h, uint64_t need_buckets, cudaStream_t s) {
         (e = cudaMemcpyAsync(nbase + c.fbits, obase + oc.fbits, owords * 4, cudaMemcpyDeviceToDevice, s)) !=
             cudaSuccess ||
         (e = cudaMemcpyAsync(nbase + c.ctr, obase + oc.ctr, kCounterBytes, cudaMemcpyDeviceToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(nbase + c.tags, obase + oc.tags, (size_t)nb * 8, cudaMemcpyDeviceToDevice, s)) !=
             cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess) {
         cudaFree(nblock);
@@ -1014,16 +1077,13 @@ int hive_clear(hive_table* h, void* stream) {
     } while (0)
 
 // Launch a two-pass kernel: the first pass with deferral when the queue exists, else one pass.
-// HIVE_DISPATCH_DM names the mode of a deferring first pass on a table without holes.
-#define HIVE_DISPATCH_D(kern, d, grid, block, stream, ...) \
-    HIVE_DISPATCH_DM(kern, hive::kModeMono, d, grid, block, stream, __VA_ARGS__)
-#define HIVE_DISPATCH_DM(kern, mono, d, grid, block, stream, ...)                            \
+#define HIVE_DISPATCH_D(kern, d, grid, block, stream, ...)                                  \
     do {                                                                                   \
         const bool p1_ = h->policy == HIVE_POLICY_MURMURCITYHASH;                          \
         const bool holes_ = h->t.flags & hive::kFlagHoles;                                 \
         if (d.q && !holes_) {                                                              \
-            if (p1_) kern<1, true, mono><<<grid, block, 0, stream>>>(__VA_ARGS__);             \
-            else kern<0, true, mono><<<grid, block, 0, stream>>>(__VA_ARGS__);                 \
+            if (p1_) kern<1, true, hive::kModeMono><<<grid, block, 0, stream>>>(__VA_ARGS__);  \
+            else kern<0, true, hive::kModeMono><<<grid, block, 0, stream>>>(__VA_ARGS__);      \
         } else if (d.q) {                                                                  \
             if (p1_) kern<1, true, hive::kModeHoles><<<grid, block, 0, stream>>>(__VA_ARGS__); \
             else kern<0, true, hive::kModeHoles><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
@@ -1032,6 +1092,68 @@ int hive_clear(hive_table* h, void* stream) {
             else kern<0, false, hive::kModeRuntime><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
         }                                                                                  \
     } while (0)
+
+}  // extern "C"
+
+namespace {
+
+// Tag upkeep of a bulk insert of n ops: per op, or none during its launches and one rebuild of
+// the tag words after them (HIVE_TUNE_BULK_RETAG: 0 never, 1 when the batch holds at least one
+// op per eight buckets, 2 always).  Per-op upkeep is a random L2 atomic on the tag words, which
+// the insert's own dirty slot sectors push out of L2; a rebuild streams the slots once.
+bool bulk_untagged(const hive_table* h, uint64_t n) {
+    const int64_t m = h->tune[HIVE_TUNE_BULK_RETAG];
+    return m == 2 || (m == 1 && n * 8 >= num_buckets(h));
+}
+
+// The Table copy a bulk insert launches with.
+hive::Table insert_view(const hive_table* h, bool untagged) {
+    hive::Table t = h->t;
+    if (untagged) t.flags |= hive::kFlagUntagged;
+    return t;
+}
+
+// First pass of an insert (k_insert) over ops [lo, hi): deferring when the queue exists, with
+// the mode bits kExtra on top of the table's base mode.
+template <int kExtra>
+void first_pass(const hive_table* h, const hive::Table& t, const Defer& d, unsigned grid, cudaStream_t s,
+                const uint32_t* keys, const uint32_t* vals, uint64_t lo, uint64_t hi, uint8_t* status) {
+    const bool p1 = h->policy == HIVE_POLICY_MURMURCITYHASH;
+    const bool holes = t.flags & hive::kFlagHoles;
+    if (d.q && !holes) {
+        if (p1) k_insert<1, true, hive::kModeMono | kExtra><<<grid, kBlock, 0, s>>>(t, keys, vals, lo, hi, status, d);
+        else k_insert<0, true, hive::kModeMono | kExtra><<<grid, kBlock, 0, s>>>(t, keys, vals, lo, hi, status, d);
+    } else if (d.q) {
+        if (p1) k_insert<1, true, hive::kModeHoles | kExtra><<<grid, kBlock, 0, s>>>(t, keys, vals, lo, hi, status, d);
+        else k_insert<0, true, hive::kModeHoles | kExtra><<<grid, kBlock, 0, s>>>(t, keys, vals, lo, hi, status, d);
+    } else {
+        if (p1) k_insert<1, false, hive::kModeRuntime | kExtra><<<grid, kBlock, 0, s>>>(t, keys, vals, lo, hi, status, d);
+        else k_insert<0, false, hive::kModeRuntime | kExtra><<<grid, kBlock, 0, s>>>(t, keys, vals, lo, hi, status, d);
+    }
+}
+
+// primary: claim in H0 only in the first pass (region-ordered batches).
+void launch_first_pass(const hive_table* h, const hive::Table& t, const Defer& d, uint64_t lo, uint64_t hi,
+                       cudaStream_t s, const uint32_t* keys, const uint32_t* vals, uint8_t* status, bool primary) {
+    const unsigned grid = grid_for(hi - lo);
+    if (t.flags & hive::kFlagUntagged) {
+        if (primary) first_pass<hive::kModeUntagged | hive::kModePrimary>(h, t, d, grid, s, keys, vals, lo, hi, status);
+        else first_pass<hive::kModeUntagged>(h, t, d, grid, s, keys, vals, lo, hi, status);
+    } else {
+        if (primary) first_pass<hive::kModePrimary>(h, t, d, grid, s, keys, vals, lo, hi, status);
+        else first_pass<0>(h, t, d, grid, s, keys, vals, lo, hi, status);
+    }
+}
+
+// Rebuild the tag words of the buckets in use from their slots (after an untagged bulk insert).
+void retag(const hive_table* h, cudaStream_t s) {
+    const uint64_t nb = num_buckets(h);
+    k_retag<<<grid_for(nb), kBlock, 0, s>>>(h->t, nb);
+}
+
+}  // namespace
+
+extern "C" {
 
 int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uint64_t n, uint8_t* status,
                 void* stream) {
@@ -1043,6 +1165,8 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
     Defer d;
     int rc = prepare_defer(h, n, s, &d);
     if (rc) return rc;
+    const bool untag = bulk_untagged(h, n);
+    const hive::Table tt = insert_view(h, untag);
     if (use_regions(h, n, HIVE_TUNE_REGION_INSERT)) {
         // region-ordered: sort, both passes over the sorted arrays, statuses back to caller order
         Regions r;
@@ -1055,17 +1179,18 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
             if (!m) continue;
             if (k && (rc = prepare_defer(h, m, s, &d))) return rc;
             uint8_t* rst = status ? r.rst + lo : nullptr;
-            HIVE_DISPATCH_DM(k_insert, hive::kModeMonoPrimary, d, grid_for(m), kBlock, s, h->t, r.rkeys + lo, r.rvals + lo,
-                             0, m, rst, d);
+            launch_first_pass(h, tt, d, 0, m, s, r.rkeys + lo, r.rvals + lo, rst, true);
             if (d.q)
-                HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, m), kBlock, s, h->t, r.rkeys + lo, r.rvals + lo, rst,
+                HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, m), kBlock, s, tt, r.rkeys + lo, r.rvals + lo, rst,
                               d);
         }
+        if (untag) retag(h, s);
         if (status) k_unpermute_u8<<<grid_for(n), kBlock, 0, s>>>(r.ridx, r.rst, n, status);
         return launch_check();
     }
-    HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, 0, n, status, d);
-    if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, d);
+    launch_first_pass(h, tt, d, 0, n, s, keys, values, status, false);
+    if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, tt, keys, values, status, d);
+    if (untag) retag(h, s);
     return launch_check();
 }
 
@@ -1116,8 +1241,11 @@ int hive_insert_noalloc(hive_table* h, const uint32_t* keys, const uint32_t* val
     cudaStream_t s = (cudaStream_t)stream;
     Defer d{base + kNoAllocHeaderWords, (u64*)base};
     HIVE_CUDA(cudaMemsetAsync(d.n, 0, sizeof(u64), s));  // the queue count must start at zero
-    HIVE_DISPATCH_D(k_insert, d, grid_for(n), kBlock, s, h->t, keys, values, 0, n, status, d);
-    HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, d);
+    const bool untag = bulk_untagged(h, n);
+    const hive::Table tt = insert_view(h, untag);
+    launch_first_pass(h, tt, d, 0, n, s, keys, values, status, false);
+    HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, tt, keys, values, status, d);
+    if (untag) retag(h, s);
     return launch_check();
 }
 
@@ -1206,15 +1334,18 @@ int hive_insert_host(hive_table* h, const uint32_t* keys, const uint32_t* values
     if ((rc = prepare_pipe(h, n, &st)) || (rc = prepare_defer(h, n, s, &d))) return rc;
     HIVE_CUDA(cudaStreamWaitEvent(h->pipe_h2d, h->ev_ins_free, 0));
     uint8_t* dst = status ? st.ist : nullptr;
+    const bool untag = bulk_untagged(h, n);
+    const hive::Table tt = insert_view(h, untag);
     for (uint64_t lo = 0; lo < n; lo += kPipeChunk) {
         const uint64_t m = std::min(kPipeChunk, n - lo);
         HIVE_CUDA(cudaMemcpyAsync(st.ik + lo, keys + lo, m * 4, cudaMemcpyHostToDevice, h->pipe_h2d));
         HIVE_CUDA(cudaMemcpyAsync(st.iv + lo, values + lo, m * 4, cudaMemcpyHostToDevice, h->pipe_h2d));
         HIVE_CUDA(order(h->ev_in, h->pipe_h2d, s));
         // first pass of this chunk; its deferred ops join the batch's one queue
-        HIVE_DISPATCH_D(k_insert, d, grid_for(m), kBlock, s, h->t, st.ik, st.iv, lo, lo + m, dst, d);
+        launch_first_pass(h, tt, d, lo, lo + m, s, st.ik, st.iv, dst, false);
     }
-    if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, h->t, st.ik, st.iv, dst, d);
+    if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, tt, st.ik, st.iv, dst, d);
+    if (untag) retag(h, s);
     if (status) {
         HIVE_CUDA(order(h->ev_out, s, h->pipe_d2h));
         HIVE_CUDA(cudaMemcpyAsync(status, st.ist, n, cudaMemcpyDeviceToHost, h->pipe_d2h));
@@ -1429,9 +1560,25 @@ int hive_counters(hive_table* h, uint64_t* out, void* stream) {
     return HIVE_OK;
 }
 
+int hive_verify(hive_table* h, uint64_t* out, void* stream) {
+    if (!valid_table(h) || !out) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    if (!g.ok) return HIVE_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    u64* d = h->scratch + 2;  // scratch words 2..5
+    HIVE_CUDA(cudaMemsetAsync(d, 0, HIVE_VERIFY_COUNT * 8, s));
+    const uint64_t nb = num_buckets(h);
+    HIVE_DISPATCH(k_verify, grid_for(nb), kBlock, s, h->t, nb, !(h->t.flags & hive::kFlagHoles), d);
+    int rc = launch_check();
+    if (rc) return rc;
+    HIVE_CUDA(cudaMemcpyAsync(out, d, HIVE_VERIFY_COUNT * 8, cudaMemcpyDeviceToHost, s));
+    HIVE_CUDA(cudaStreamSynchronize(s));
+    return HIVE_OK;
+}
+
 int hive_set_tuning(hive_table* h, int32_t key, int64_t value) {
     if (!valid_table(h) || key < 0 || key >= HIVE_NUM_TUNES) return HIVE_ERR_INVALID_ARG;
-    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1}, hi[HIVE_NUM_TUNES] = {1, 1, 8, 8};
+    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0}, hi[HIVE_NUM_TUNES] = {1, 1, 8, 8, 2};
     if (value < lo[key] || value > hi[key]) return HIVE_ERR_INVALID_ARG;
     h->tune[key] = value;
     return HIVE_OK;

@@ -37,7 +37,7 @@ NUM_COUNTERS = 16
 COUNTER_NAMES = {0: "slow_path", 1: "evictions", 2: "stash_push", 3: "failed", 4: "lock_timeout",
                  5: "retry_out", 6: "dup_fixed", 15: "error_bits"}
 # Launch-tuning knobs (HIVE_TUNE_*): how a batch runs, never what it computes
-TUNES = {"region_insert": 0, "region_find": 1, "subbatches": 2, "second_pass_blocks": 3}
+TUNES = {"region_insert": 0, "region_find": 1, "subbatches": 2, "second_pass_blocks": 3, "bulk_retag": 4}
 
 # Policy names accepted by the reference's dispatcher (src/hive_dispatch.cu:829-871).  The
 # ones outside the hot path fall back to Default2Hash with a message, as the reference does for
@@ -92,6 +92,7 @@ ABI = [
     ("hive_get_info", _I32, [_P, ctypes.POINTER(Info)]),
     ("hive_counters", _I32, [_P, _P, _P]),
     ("hive_check", _I32, [_P, _P]),
+    ("hive_verify", _I32, [_P, _P, _P]),
     ("hive_set_tuning", _I32, [_P, _I32, ctypes.c_int64]),
     ("hive_get_tuning", _I32, [_P, _I32, ctypes.POINTER(ctypes.c_int64)]),
     ("hive_strerror", ctypes.c_char_p, [_I32]),
@@ -369,6 +370,13 @@ class HiveHashTable:
 
     def check(self, stream=None) -> None:
         _check(self._lib.hive_check(self._h, self._stream(stream)), "hive_check")
+
+    def verify(self, stream=None) -> dict:
+        """Structural check on the device (hive_verify): violation counts, all 0 when sound."""
+        buf = (ctypes.c_uint64 * 4)()
+        _check(self._lib.hive_verify(self._h, ctypes.cast(buf, ctypes.c_void_p), self._stream(stream)),
+               "hive_verify")
+        return {name: int(buf[i]) for i, name in enumerate(("tag_mismatch", "misplaced", "duplicate", "stale_tag"))}
 
     def set_tuning(self, **knobs) -> None:
         """set_tuning(region_insert=1, subbatches=4, ...): see TUNES."""

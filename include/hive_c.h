@@ -234,6 +234,20 @@ int hive_counters(hive_table* t, uint64_t* out, void* stream);
  * include/hive_hash_table_struct.cuh:101-117). */
 int hive_check(hive_table* t, void* stream);
 
+/* Structural check of the table on the device (synchronises `stream`): out[HIVE_VERIFY_*] counts
+ * slots whose per-slot fingerprint byte is not their key's, keys outside both of their buckets
+ * (stash entries outside their canonical bucket's stash), keys held twice in one bucket, and --
+ * on a table with no delete or resize since the last clear -- free slots with a nonzero
+ * fingerprint.  All zero on a sound table.  Replaces the reference's post-run table checks
+ * (count_occupancy_kernel, src/hive_dispatch.cu:169-176; freeMask copy-back,
+ * src/hive_dispatch.cu:1023-1036), which count occupancy only. */
+#define HIVE_VERIFY_TAG_MISMATCH 0
+#define HIVE_VERIFY_MISPLACED 1
+#define HIVE_VERIFY_DUPLICATE 2
+#define HIVE_VERIFY_STALE_TAG 3
+#define HIVE_VERIFY_COUNT 4
+int hive_verify(hive_table* t, uint64_t* out, void* stream);
+
 /* ---- launch tuning (hive_set_tuning / hive_get_tuning) ----------------------------------------
  * Knobs of how a batch is run, never of what it computes: every setting gives the results of
  * the one-at-a-time replay.  They replace the reference's compile-time launch constants
@@ -246,7 +260,11 @@ int hive_check(hive_table* t, void* stream);
                                         = chosen from the share of the capacity the batch adds   */
 #define HIVE_TUNE_SECOND_PASS_BLOCKS 3 /* resident blocks per SM of the second insert pass, 1..8;
                                           default 4                                             */
-#define HIVE_NUM_TUNES 4
+#define HIVE_TUNE_BULK_RETAG 4       /* per-slot fingerprint upkeep of hive_insert*: 0 per op; 1
+                                        (default) per op for batches under one op per eight
+                                        buckets, else one rebuild of the fingerprints after the
+                                        batch; 2 always the rebuild                              */
+#define HIVE_NUM_TUNES 5
 
 /* Set knob `key` to `value`.  HIVE_ERR_INVALID_ARG for an unknown key or a value out of range. */
 int hive_set_tuning(hive_table* t, int32_t key, int64_t value);

@@ -32,6 +32,8 @@ def _replay_and_check(run, wl, runner, table):
     np.testing.assert_array_equal(gk, ok)
     np.testing.assert_array_equal(gv, ov)
     assert len(m) == wl.final_live
+    v = table.verify()
+    assert v["tag_mismatch"] == v["misplaced"] == v["duplicate"] == 0, v
 
 
 @pytest.mark.parametrize("policy", ["Default2Hash", "MurmurCityHash"])

@@ -30,6 +30,8 @@ def _assert_same_set(table: HiveHashTable, m: oracle.ReplayMap):
     np.testing.assert_array_equal(gk, ok)
     np.testing.assert_array_equal(gv, ov)
     assert table.size() == len(m)
+    # fingerprints, placement, no duplicates (and no stale fingerprints without holes)
+    assert table.verify() == {"tag_mismatch": 0, "misplaced": 0, "duplicate": 0, "stale_tag": 0}
 
 
 def _insert_and_check(table, m, keys, vals):
@@ -179,10 +181,40 @@ def test_host_buffer_calls(cuda, pinned):
         t.check()
 
 
+@pytest.mark.parametrize("policy", POLICIES)
+@pytest.mark.parametrize("retag", [0, 2])
+def test_tag_upkeep_modes(cuda, policy, retag):
+    """Per-slot fingerprints kept per op (0) or rebuilt after each bulk insert (2): the same
+    results as the replay through bulk insert, updates, erases and re-inserts, and the
+    fingerprint invariant holds after every step."""
+    cap = 1 << 20
+    n = int(0.92 * cap)
+    keys, absent, st = oracle.gen_keys(23, n, 1 << 15)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(cap, policy) as t:
+        t.set_tuning(bulk_retag=retag)
+        ins = _insert_and_check(t, m, keys, vals)
+        assert (ins != ST_FAIL).all()
+        _assert_same_set(t, m)
+        upd = keys[::5].copy()
+        _insert_and_check(t, m, upd, oracle.values_for(upd) + np.uint32(9))
+        gone = keys[1::3].copy()
+        st_e = _np(t.erase(gone))
+        np.testing.assert_array_equal(st_e, m.erase(gone))
+        _assert_same_set(t, m)
+        _insert_and_check(t, m, gone[::2].copy(), oracle.values_for(gone[::2]))
+        look, _ = oracle.lookup_set(keys, absent, 1 << 15, 1 << 15, st)
+        _find_and_check(t, m, look)
+        _assert_same_set(t, m)
+        t.check()
+
+
 def test_tuning_bounds(cuda):
     with HiveHashTable(1 << 12) as t:
-        assert t.tuning() == {"region_insert": 0, "region_find": 0, "subbatches": 0, "second_pass_blocks": 4}
-        for bad in ({"region_insert": 2}, {"subbatches": 9}, {"second_pass_blocks": 0}):
+        assert t.tuning() == {"region_insert": 0, "region_find": 0, "subbatches": 0, "second_pass_blocks": 4,
+                              "bulk_retag": 1}
+        for bad in ({"region_insert": 2}, {"subbatches": 9}, {"second_pass_blocks": 0}, {"bulk_retag": 3}):
             with pytest.raises(HiveError):
                 t.set_tuning(**bad)
         t.set_tuning(second_pass_blocks=8)
@@ -414,4 +446,5 @@ def test_full_size_properties(cuda):
         assert gk.size == n and np.unique(gk).size == n
         assert int(gk.astype(np.uint64).sum()) == int(keys.astype(np.uint64).sum())
         assert int(gv.astype(np.uint64).sum()) == int(vals.astype(np.uint64).sum())
+        assert t.verify() == {"tag_mismatch": 0, "misplaced": 0, "duplicate": 0, "stale_tag": 0}
         t.check()

@@ -37,6 +37,8 @@ def test_served_results_equal_arrival_order_replay(cuda, mix, depth, rate):
         ok, ov = m.dump()
         np.testing.assert_array_equal(gk, ok)
         np.testing.assert_array_equal(gv, ov)
+        v = t.verify()
+        assert v["tag_mismatch"] == v["misplaced"] == v["duplicate"] == 0, v
         t.check()
 
 
