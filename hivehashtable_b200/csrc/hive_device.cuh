@@ -350,9 +350,23 @@ __device__ __forceinline__ u64 ld_relaxed_u64(const u64* p) {
     return v;
 }
 __device__ __forceinline__ u64 load_tags(const Table& t, uint32_t b) { return ld_relaxed_u64(t.tags + b); }
+// L2 cache policies of the read-only lookup path: the tag words (reused by every lookup) are
+// kept in L2 ahead of the slot sectors, each of which a lookup batch touches about once.
+__device__ __forceinline__ u64 l2_evict_last() {
+    u64 p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ u64 l2_evict_first() {
+    u64 p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
 __device__ __forceinline__ u64 load_tags_ro(const Table& t, uint32_t b) {
     u64 v;
-    asm volatile("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(t.tags + b));
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u64 %0, [%1], %2;"
+                 : "=l"(v)
+                 : "l"(t.tags + b), "l"(l2_evict_last()));
     return v;
 }
 
@@ -417,9 +431,9 @@ struct Sector {
     u64 s[4];
 };
 __device__ __forceinline__ void load_sector_ro(const u64* p, Sector& S) {
-    asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u64 {%0,%1,%2,%3}, [%4], %5;"
                  : "=l"(S.s[0]), "=l"(S.s[1]), "=l"(S.s[2]), "=l"(S.s[3])
-                 : "l"(p));
+                 : "l"(p), "l"(l2_evict_first()));
 }
 __device__ __forceinline__ void load_sector(const u64* p, Sector& S) {
     asm volatile("ld.relaxed.gpu.global.v4.u64 {%0,%1,%2,%3}, [%4];"
