@@ -164,6 +164,29 @@ def random_bucket_ceiling(dev, table_bytes):
     return out
 
 
+def pcie_bandwidth(dev, nbytes=256 << 20, reps=4):
+    """Plain page-locked copies of nbytes each way (torch copy_, one direction at a time): the
+    transfer rates that bound the host-buffer (e2e) step."""
+    import torch
+
+    h = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    s = torch.cuda.current_stream(dev)
+    out = {}
+    for name, fn in (("h2d_gbs", lambda: d.copy_(h, non_blocking=True)),
+                     ("d2h_gbs", lambda: h.copy_(d, non_blocking=True))):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(reps):
+            fn()
+        b.record(s)
+        torch.cuda.synchronize()
+        out[name] = round(reps * nbytes / (a.elapsed_time(b) / 1e3) / 1e9, 1)
+    return out
+
+
 def cpu_baseline(args, threads=None):
     """The CPU port of the same algorithm (oracle/hive_oracle.cpp) on every host core: a bounded
     sample with the headline's LF and present fraction at 2^cpu_sample_log slots."""
@@ -339,7 +362,11 @@ def main():
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             ems = float(tt.item())
         assert int(fd_h.sum()) == n_present and int((st_h != 0).sum()) == n
+        pcie = pcie_bandwidth(dev)
+        h2d_bound_ms = (n * 8 + n_look * 4) / (pcie["h2d_gbs"] * 1e9) * 1e3
         e2e = {"value": round(2 * n * args.steps * world / (ems / 1e3) / 1e6, 2), "unit": UNIT,
+               "pcie": pcie, "h2d_bound_ms": round(h2d_bound_ms, 3),
+               "frac_of_h2d_bound": round(h2d_bound_ms / (ems / args.steps), 4),
                "h2d_bytes_per_step": int(n * 8 + n_look * 4), "d2h_bytes_per_step": int(n + n_look * 5),
                "ms_per_step": round(ems / args.steps, 4), "api": "HiveHashTable.insert_host + find_host",
                "gpu_launches_per_step": 1 + -(-n // (1 << 22)) + 2 + -(-n_look // (1 << 22))}
