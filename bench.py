@@ -41,8 +41,10 @@ BYTES_INSERT = 172.0
 BYTES_LOOKUP_PRESENT = 76.0
 BYTES_LOOKUP_ABSENT = 140.0
 # DRAM bytes per op measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum per launch / ops)
-# for k_insert and k_find at this workload; profiles/k_insert_k_find_ncu_2p26_lf09.txt.
-TRAFFIC_PER_OP = {"insert": None, "lookup": None}
+# at this workload (2^26 slots, LF 0.9, Default2Hash): the insert's three launches (first pass,
+# deferred pass, fingerprint rebuild) and k_find; profiles/bulk_insert_lookup_2p26_dram_traffic.txt.
+# A measurement of this build: re-capture after a change to either kernel.
+TRAFFIC_PER_OP = {"insert": 206.4, "lookup": 99.5}
 
 
 def parse_args():
@@ -60,6 +62,10 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-bucket ceiling probes")
     ap.add_argument("--cpu-sample-log", type=int, default=24, help="log2 slots of the CPU-baseline sample")
+    ap.add_argument("--workload", choices=["bulk", "batched", "served", "resize"], default="bulk",
+                    help="bulk: the headline (default); the others run one GPU and print their own line")
+    ap.add_argument("--batches", type=int, default=4096, help="batched: number of mixed batches")
+    ap.add_argument("--requests-log", type=int, default=22, help="served: log2 requests per run")
     return ap.parse_args()
 
 
@@ -232,6 +238,152 @@ def run_reference(args, rank, world):
     return line
 
 
+def _events(stream, fn):
+    import torch
+
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    out = fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b), out
+
+
+def run_batched(args, dev):
+    """Mixed batches (seed 11): a 2^24-slot table prefilled to LF 0.7, then `batches` batches of
+    floor(2^U) ops, U ~ Uniform[10, 20): 50 % inserts of new keys, 40 % lookups (80 % present),
+    10 % deletes; the table grows by linear-hashing doubling before a batch that would pass LF 0.85.
+    One hive_apply_ops call per batch (plain) against hive_apply_batches (persistent cooperative
+    kernel with a grid barrier between batches, one launch per growth segment)."""
+    from hivehashtable_b200 import HiveHashTable
+    from hivehashtable_b200.batched import BatchedRunner
+    from hivehashtable_b200.workload import MixedWorkload
+
+    wl = MixedWorkload(11, int(0.7 * (1 << 24)), args.batches, 10.0, 20.0)
+    out = {"metric": "batched mixed ops Mops/s (50/40/10 insert/lookup/delete, growth included)", "unit": "Mops/s",
+           "workload": f"2^24 slots prefilled to LF 0.7, {args.batches} batches of 2^U ops (U~U[10,20)), "
+                       f"{wl.total_ops:,} ops, {wl.final_live:,} live keys at the end",
+           "higher_is_better": True}
+    for mode in ("plain", "persistent"):
+        with HiveHashTable(1 << 24, max_capacity=1 << 29) as t:
+            r = BatchedRunner(t, wl, max_load=0.85)
+            r.prefill()
+            torch_sync()
+            res = r.run_plain() if mode == "plain" else r.run_persistent()
+            st = r.status.cpu().numpy()
+            ins_failed = int(((wl.types == 0) & (st == 0)).sum())
+            out[mode] = {"mops": round(res.mops, 1), "ms": round(res.ms, 3), "launch_calls": res.launches,
+                         "resizes": res.resizes, "final_capacity_slots": t.info()["capacity_slots"],
+                         "size_ok": t.size() == wl.final_live, "inserts_failed": ins_failed}
+            t.check()
+        del r
+    out["value"] = out["persistent"]["mops"]
+    return out
+
+
+def torch_sync():
+    import torch
+
+    torch.cuda.synchronize()
+
+
+def run_served(args, dev):
+    """Served requests (seed 17): 2^26 records preloaded into 2^27 slots, keys Zipf(0.99) over the
+    records, mixes A (50/50 lookup/update), B (95/5), C (lookups), D (95 % lookups, 5 % new
+    inserts); the C++ serving loop (hive_serve_run) batches arrivals by arrival time.  Per mix: the
+    closed-loop peak (every request present at t = 0), then Poisson arrivals at fractions of that
+    peak with p50/p99/p999 of arrival -> result on the host."""
+    from hivehashtable_b200 import HiveHashTable
+    from hivehashtable_b200.serving import ServedWorkload, poisson_arrivals, serve
+
+    n_req = 1 << args.requests_log
+    out = {"metric": "served requests: latency p50/p99/p999 (ms) at fractions of peak Mops/s", "unit": "ms",
+           "workload": f"2^26 records in 2^27 slots, Zipf 0.99, {n_req:,} requests per run, depth 4, batches <= 2^16",
+           "higher_is_better": False, "mixes": {}}
+    for mix in ("A", "B", "C", "D"):
+        w = ServedWorkload(17, 1 << 26, n_req, mix)
+        with HiveHashTable(1 << 27) as t:
+            st = t.insert(w.preload_keys, w.preload_vals)
+            torch_sync()
+            assert bool((st != 0).all())
+            r = serve(t, w.types, w.keys, w.vals, poisson_arrivals(n_req, 0), depth=4, max_batch=1 << 16)
+            peak = r.summary()["mops"]
+            runs = {"peak": {k: round(v, 4) if isinstance(v, float) else v for k, v in r.summary().items()}}
+            for frac in (0.1, 0.25, 0.5, 0.75, 0.9):
+                arr = poisson_arrivals(n_req, frac * peak * 1e6, seed=int(frac * 100))
+                s = serve(t, w.types, w.keys, w.vals, arr, depth=4, max_batch=1 << 16).summary()
+                runs[f"{frac:.2f}"] = {k: round(s[k], 4) for k in ("mops", "p50_ms", "p99_ms", "p999_ms")}
+            out["mixes"][mix] = runs
+            t.check()
+    return out
+
+
+def run_resize(args, dev):
+    """Growth and shrink (seed 13): a 2^20-slot table takes 2^27 unique keys in 128 chunks of
+    2^20 inserts, each followed by 2^17 lookups of inserted keys, doubling (linear-hashing splits)
+    before a chunk would pass LF 0.85; then 75 % of the keys are deleted in random order in chunks of
+    2^20, shrinking to LF 0.75 whenever the load falls below 0.25.  Device time of each phase with
+    its resizes included."""
+    import numpy as np
+    import torch
+    from hivehashtable_b200 import HiveHashTable, as_device_u32
+    from hivehashtable_b200 import workload
+
+    n, chunk = 1 << 27, 1 << 20
+    keys, _, _ = workload.gen_keys(13, n, 0)
+    vals = workload.values_for(keys)
+    order = np.arange(n, dtype=np.int64)
+    np.random.default_rng(13).shuffle(order)
+    kd, vd = as_device_u32(keys, dev), as_device_u32(vals, dev)
+    gone = as_device_u32(keys[order[: 3 * n // 4]], dev)
+    look_idx = torch.from_numpy(np.random.default_rng(14).integers(0, chunk, size=chunk // 8)).to(dev)
+    looks = kd.view(-1, chunk)[:, look_idx].contiguous()  # 2^17 inserted keys per chunk
+    stream = torch.cuda.current_stream(dev)
+    out = {"metric": "resize: inserts with growth, deletes with shrink (Mops/s)", "unit": "Mops/s",
+           "workload": "2^20 slots -> 2^27 keys in 128 chunks of 2^20 (+2^17 lookups each); delete 75 % in chunks",
+           "higher_is_better": True}
+    with HiveHashTable(1 << 20, max_capacity=1 << 29) as t:
+        grows = 0
+        missing = torch.zeros((), dtype=torch.int64, device=dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for c in range(n // chunk):
+            live = c * chunk
+            cap = t.info()["capacity_slots"]
+            while (live + chunk) > 0.85 * cap:
+                cap *= 2
+            if cap != t.info()["capacity_slots"]:
+                t.resize(cap)
+                grows += 1
+            t.insert(kd[c * chunk:(c + 1) * chunk], vd[c * chunk:(c + 1) * chunk])
+            _, f = t.find(looks[c])
+            missing += (f == 0).sum()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ins_ms = a.elapsed_time(b)
+        size_after_insert = t.size()
+        shrinks = 0
+        a.record(stream)
+        for c in range(0, gone.numel(), chunk):
+            t.erase(gone[c:c + chunk])
+            live = n - min(c + chunk, gone.numel())
+            cap = t.info()["capacity_slots"]
+            if live < 0.25 * cap:
+                t.resize(max(int(live / 0.75) // 8 * 8, 1 << 20))
+                shrinks += 1
+        b.record(stream)
+        torch.cuda.synchronize()
+        del_ms = a.elapsed_time(b)
+        out.update({"insert_mops": round(n / ins_ms / 1e3, 1), "insert_ms": round(ins_ms, 2), "grows": grows,
+                    "lookups_missing": int(missing.item()), "size_after_insert": size_after_insert,
+                    "delete_mops": round(gone.numel() / del_ms / 1e3, 1), "delete_ms": round(del_ms, 2),
+                    "shrinks": shrinks, "size_after_delete": t.size(),
+                    "final_capacity_slots": t.info()["capacity_slots"]})
+        out["value"] = out["insert_mops"]
+        t.check()
+    return out
+
+
 def workload_config(args, world, note=None):
     cap = 1 << args.cap_log
     n = int(args.lf * cap)
@@ -263,6 +415,13 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.workload != "bulk":
+        if rank == 0:
+            fn = {"batched": run_batched, "served": run_served, "resize": run_resize}[args.workload]
+            line = fn(args, dev)
+            line.update({"n_gpus": 1, "data": "synthetic", "dtype": "u32"})
+            print(json.dumps(line), flush=True)
+        return
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
@@ -396,13 +555,16 @@ def main():
                         "algorithmic_bytes": kd["bytes"], "ms_per_launch": round(kd["ms"], 4),
                         "mops": round(kd["ops"] / kd["ms"] / 1e3, 1)}
         if ceiling:
-            # the same ops at the probe's raw access rate: insert = one bucket read + CAS;
-            # lookup = one read when present, two dependent reads when absent
+            # the same ops at the probe's raw access rate: insert = one bucket read + CAS; lookup =
+            # one random 32 B sector per present key (fingerprint words are L2 hits and an absent
+            # key reads no slot)
             ins_ceiling = ceiling["read64_cas_table"]["gops"]
-            p = args.present
-            look_ceiling = 1.0 / (p / ceiling["read64_table"]["gops"] + (1 - p) / ceiling["read64x2_table"]["gops"])
+            p = max(args.present, 1e-9)
+            look_ceiling = ceiling["read32_table"]["gops"] / p
             rl["k_insert"]["frac_of_probe_ops"] = round(rl["k_insert"]["mops"] / 1e3 / ins_ceiling, 4)
             rl["k_find"]["frac_of_probe_ops"] = round(rl["k_find"]["mops"] / 1e3 / look_ceiling, 4)
+        rl["k_insert"]["launches"] = ["k_insert", "k_insert_deferred", "k_retag"]
+        rl["k_find"]["launches"] = ["k_find"]
         dom = max(kernels, key=lambda k: kernels[k]["ms"])
         roof = dict(rl[dom], kernel=dom)
         line = {"metric": METRIC, "value": round(2 * n * args.steps * world / (ms / 1e3) / 1e6, 2), "unit": UNIT,
