@@ -10,8 +10,9 @@ and is larger than the 126 MB L2 (table 512 MiB, key arrays 241 MB each).
 `e2e` times the same step through the public host-buffer API (HiveHashTable.insert_host /
 find_host over hive_insert_host / hive_find_host) from pinned host buffers, with the host->device
 copies of keys/values/lookup keys and the device->host copies of statuses/found flags/values
-inside the timed region (the library overlaps them with the table work in 2^22-op chunks).  `cpu_baseline` / `--impl reference` time the CPU port of the same
-algorithm (oracle/hive_oracle.cpp, std::thread on every host core) on a bounded sample.
+inside the timed region (the library overlaps them with the table work in 2^22-op chunks).
+`cpu_baseline` / `--impl reference` time the CPU port of the same algorithm
+(oracle/hive_oracle.cpp, std::thread on every host core) on a bounded sample.
 
 Multi-GPU (torchrun): each rank owns an independent table with its own keys (seed 7 + 1000*rank);
 there is no data-path collective, so scaling is weak.
