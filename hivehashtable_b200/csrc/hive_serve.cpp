@@ -28,8 +28,6 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
-#include <deque>
-#include <unordered_map>
 #include <vector>
 
 #include "hive_serve.h"
@@ -37,6 +35,55 @@
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+// Key -> group index of one batch: open addressing with linear probing over a power-of-two table
+// at least twice the batch size.  A slot belongs to the current batch iff its stamp equals the
+// batch's generation, so starting a batch costs one increment instead of a clear.
+class GroupMap {
+  public:
+    explicit GroupMap(uint32_t max_keys) {
+        uint32_t sz = 16;
+        while (sz < 2u * max_keys) sz <<= 1;
+        mask_ = sz - 1;
+        keys_.resize(sz);
+        vals_.resize(sz);
+        stamp_.assign(sz, 0u);
+    }
+    void next_batch() {
+        if (++gen_ == 0) {  // stamps wrapped: clear once every 2^32 batches
+            std::fill(stamp_.begin(), stamp_.end(), 0u);
+            gen_ = 1;
+        }
+    }
+    // The group of key k; *added is true when k is new to the batch (its group is then `fresh`).
+    int32_t find_or_add(uint32_t k, int32_t fresh, bool* added) {
+        uint32_t h = k;
+        h ^= h >> 16;
+        h *= 0x85ebca6bu;
+        h ^= h >> 13;
+        h *= 0xc2b2ae35u;
+        h ^= h >> 16;
+        for (uint32_t i = h & mask_;; i = (i + 1) & mask_) {
+            if (stamp_[i] != gen_) {
+                stamp_[i] = gen_;
+                keys_[i] = k;
+                vals_[i] = fresh;
+                *added = true;
+                return fresh;
+            }
+            if (keys_[i] == k) {
+                *added = false;
+                return vals_[i];
+            }
+        }
+    }
+
+  private:
+    std::vector<uint32_t> keys_;
+    std::vector<int32_t> vals_;
+    std::vector<uint32_t> stamp_;
+    uint32_t mask_ = 0, gen_ = 0;
+};
 
 struct Slot {
     cudaStream_t copy = nullptr;
@@ -47,9 +94,10 @@ struct Slot {
     // device
     uint32_t *d_fkeys = nullptr, *d_ukeys = nullptr, *d_uvals = nullptr, *d_fvals = nullptr;
     uint8_t *d_ftypes = nullptr, *d_utypes = nullptr, *d_found = nullptr, *d_ust = nullptr;
-    // the batch
-    std::vector<uint64_t> req;        // request indices, arrival order
+    // the batch: requests [first, first + count) in arrival order
+    uint64_t first = 0, count = 0;
     std::vector<int32_t> group;       // group of each request
+    std::vector<int32_t> lastw;       // group -> latest write answered so far (finish), or -1
     std::vector<int32_t> find_of;     // group -> position in the lookup list or -1
     std::vector<int32_t> upsert_of;   // group -> position in the upsert list or -1
     uint32_t nf = 0, nu = 0;
@@ -109,11 +157,11 @@ int hive_serve_run(
     hive_info info{};
     uint64_t live = cfg->live_keys;
 
-    std::unordered_map<uint32_t, int32_t> gid;
-    gid.reserve(cap * 2);
-    std::deque<uint64_t> pending;   // request indices waiting, arrival order
-    std::vector<uint32_t> g_lastw;  // group -> index (into slot.req) of its last write, or -1
-    uint64_t next = 0, finished = 0;
+    GroupMap gid(cap);
+    std::vector<uint32_t> g_key;    // group -> key
+    std::vector<uint32_t> g_lastw;  // group -> index (within the batch) of its last write, or ~0
+    // Requests are admitted in arrival order, so the pending ones are always [pend, next).
+    uint64_t pend = 0, next = 0, finished = 0;
     size_t head = 0;                // ring position of the oldest in-flight slot
     size_t in_flight = 0;
     const auto t0 = Clock::now();
@@ -121,13 +169,14 @@ int hive_serve_run(
 
     auto finish = [&](Slot& s) {
         // answers of the batch, in request order
-        std::vector<int32_t> lastw(s.find_of.size(), -1);
-        for (size_t j = 0; j < s.req.size(); ++j) {
-            const uint64_t r = s.req[j];
+        std::vector<int32_t>& lastw = s.lastw;
+        lastw.assign(s.find_of.size(), -1);
+        for (uint64_t j = 0; j < s.count; ++j) {
+            const uint64_t r = s.first + j;
             const int32_t g = s.group[j];
             if (types[r] == HIVE_OP_LOOKUP) {
                 if (lastw[g] >= 0) {
-                    out_vals[r] = vals[s.req[lastw[g]]];
+                    out_vals[r] = vals[s.first + lastw[g]];
                     out_status[r] = 1;
                 } else {
                     const int32_t f = s.find_of[g];
@@ -143,8 +192,8 @@ int hive_serve_run(
             }
         }
         const double td = now_s();
-        for (uint64_t r : s.req) done_s[r] = td;
-        finished += s.req.size();
+        std::fill(done_s + s.first, done_s + s.first + s.count, td);
+        finished += s.count;
         s.busy = false;
     };
 
@@ -163,7 +212,7 @@ int hive_serve_run(
     while (!rc && finished < n) {
         // admit arrivals
         const double tn = now_s();
-        while (next < n && arrival_s[next] <= tn) pending.push_back(next++);
+        while (next < n && arrival_s[next] <= tn) ++next;
         // retire completed batches in order
         while (in_flight) {
             Slot& s = slots[head];
@@ -175,8 +224,8 @@ int hive_serve_run(
             --in_flight;
         }
         if (rc) break;
-        if (pending.empty() || in_flight == slots.size()) {
-            if (pending.empty() && next < n && in_flight == 0) {
+        if (pend == next || in_flight == slots.size()) {
+            if (pend == next && next < n && in_flight == 0) {
                 // idle until the next arrival
                 while (now_s() < arrival_s[next]) {
                 }
@@ -185,27 +234,26 @@ int hive_serve_run(
         }
         // form a batch
         Slot& s = slots[tail];
-        const size_t take = std::min<size_t>(pending.size(), cap);
-        s.req.assign(pending.begin(), pending.begin() + take);
-        pending.erase(pending.begin(), pending.begin() + take);
-        gid.clear();
+        const uint64_t take = std::min<uint64_t>(next - pend, cap);
+        s.first = pend;
+        s.count = take;
+        pend += take;
+        gid.next_batch();
         s.group.resize(take);
         s.find_of.clear();
         s.upsert_of.clear();
         g_lastw.clear();
+        g_key.clear();
         uint64_t new_writes = 0;
-        for (size_t j = 0; j < take; ++j) {
-            const uint64_t r = s.req[j];
-            auto it = gid.find(keys[r]);
-            int32_t g;
-            if (it == gid.end()) {
-                g = (int32_t)s.find_of.size();
-                gid.emplace(keys[r], g);
+        for (uint64_t j = 0; j < take; ++j) {
+            const uint64_t r = s.first + j;
+            bool added;
+            const int32_t g = gid.find_or_add(keys[r], (int32_t)s.find_of.size(), &added);
+            if (added) {
                 s.find_of.push_back(types[r] == HIVE_OP_LOOKUP ? -2 : -1);  // -2: needs a lookup
                 s.upsert_of.push_back(-1);
                 g_lastw.push_back(0xFFFFFFFFu);
-            } else {
-                g = it->second;
+                g_key.push_back(keys[r]);
             }
             s.group[j] = g;
             if (types[r] != HIVE_OP_LOOKUP) {
@@ -216,20 +264,18 @@ int hive_serve_run(
         s.nf = s.nu = 0;
         for (size_t g = 0; g < s.find_of.size(); ++g) {
             if (s.find_of[g] == -2) {
-                s.h_fkeys[s.nf] = 0;
+                s.h_fkeys[s.nf] = g_key[g];
                 s.find_of[g] = (int32_t)s.nf++;
             } else {
                 s.find_of[g] = -1;
             }
             if (g_lastw[g] != 0xFFFFFFFFu) {
-                const uint64_t r = s.req[g_lastw[g]];
+                const uint64_t r = s.first + g_lastw[g];
                 s.h_ukeys[s.nu] = keys[r];
                 s.h_uvals[s.nu] = vals[r];
                 s.upsert_of[g] = (int32_t)s.nu++;
             }
         }
-        for (const auto& kv : gid)
-            if (s.find_of[kv.second] >= 0) s.h_fkeys[s.find_of[kv.second]] = kv.first;
         // growth: keep the load factor under max_load counting every write as a possible new key
         if (cfg->max_load > 0.0 && new_writes) {
             hive_get_info(t, &info);
