@@ -261,6 +261,13 @@ def run_batched(args, dev):
     from hivehashtable_b200.workload import MixedWorkload
 
     wl = MixedWorkload(11, int(0.7 * (1 << 24)), args.batches, 10.0, 20.0)
+    # warm-up: both paths once on a small workload (kernel loading, first allocations)
+    wu = MixedWorkload(3, 1 << 14, 16, 10.0, 14.0)
+    for mode in ("plain", "persistent"):
+        with HiveHashTable(1 << 15) as t:
+            r = BatchedRunner(t, wu, max_load=0.85)
+            r.prefill()
+            r.run_plain() if mode == "plain" else r.run_persistent()
     out = {"metric": "batched mixed ops Mops/s (50/40/10 insert/lookup/delete, growth included)", "unit": "Mops/s",
            "workload": f"2^24 slots prefilled to LF 0.7, {args.batches} batches of 2^U ops (U~U[10,20)), "
                        f"{wl.total_ops:,} ops, {wl.final_live:,} live keys at the end",
@@ -301,6 +308,10 @@ def run_served(args, dev):
     out = {"metric": "served requests: latency p50/p99/p999 (ms) at fractions of peak Mops/s", "unit": "ms",
            "workload": f"2^26 records in 2^27 slots, Zipf 0.99, {n_req:,} requests per run, depth 4, batches <= 2^16",
            "higher_is_better": False, "mixes": {}}
+    wu = ServedWorkload(5, 1 << 16, 1 << 16, "D")  # warm-up: kernel loading, first allocations
+    with HiveHashTable(1 << 17) as t:
+        t.insert(wu.preload_keys, wu.preload_vals)
+        serve(t, wu.types, wu.keys, wu.vals, poisson_arrivals(wu.keys.size, 0), depth=4, max_batch=1 << 16)
     for mix in ("A", "B", "C", "D"):
         w = ServedWorkload(17, 1 << 26, n_req, mix)
         with HiveHashTable(1 << 27) as t:
@@ -344,6 +355,15 @@ def run_resize(args, dev):
            "workload": "2^20 slots -> 2^27 keys in 128 chunks of 2^20 (+2^17 lookups each); delete 75 % in chunks",
            "higher_is_better": True}
     with HiveHashTable(1 << 20, max_capacity=1 << 29) as t:
+        # warm-up on this table, then clear: kernel loading and the table's own first allocations
+        # (deferred-op queue, merge overflow buffer)
+        t.insert(kd[:chunk], vd[:chunk])
+        t.find(looks[0])
+        t.resize(1 << 22)
+        t.erase(kd[: chunk // 2])
+        t.resize(1 << 20)
+        t.clear()
+        torch.cuda.synchronize()
         grows = 0
         missing = torch.zeros((), dtype=torch.int64, device=dev)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -7,6 +7,7 @@ mirror used by the tests and the benchmark.
 """
 from .table import (  # noqa: F401
     HINT_NO_DELETES,
+    HINT_UNIQUE_KEYS,
     OP_DELETE,
     OP_INCREMENT,
     OP_INSERT,

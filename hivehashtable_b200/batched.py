@@ -20,7 +20,7 @@ from typing import List, Optional
 import numpy as np
 import torch
 
-from .table import HiveHashTable, as_device_u32, as_device_u8, library
+from .table import HINT_UNIQUE_KEYS, HiveHashTable, as_device_u32, as_device_u8, library
 from .workload import MixedWorkload
 
 
@@ -39,8 +39,11 @@ class RunResult:
 
 
 class BatchedRunner:
-    def __init__(self, table: HiveHashTable, wl: MixedWorkload, max_load: float = 0.85):
-        self.t, self.wl, self.max_load = table, wl, max_load
+    """hints: HIVE_HINT_* passed with every batch.  The workload generator puts each key in at
+    most one op of a batch, so HINT_UNIQUE_KEYS holds by construction and is the default."""
+
+    def __init__(self, table: HiveHashTable, wl: MixedWorkload, max_load: float = 0.85, hints: int = HINT_UNIQUE_KEYS):
+        self.t, self.wl, self.max_load, self.hints = table, wl, max_load, hints
         dev = table.device
         self.types = as_device_u8(wl.types, dev)
         self.keys = as_device_u32(wl.keys, dev)
@@ -99,7 +102,8 @@ class BatchedRunner:
             lo, n = int(offs[bi]), int(offs[bi + 1] - offs[bi])
             if n == 0:
                 continue
-            rc = lib.hive_apply_ops(h, tp + lo, kp + 4 * lo, vp + 4 * lo, n, sp + lo, op + 4 * lo, 0, s.cuda_stream)
+            rc = lib.hive_apply_ops(h, tp + lo, kp + 4 * lo, vp + 4 * lo, n, sp + lo, op + 4 * lo, self.hints,
+                                    s.cuda_stream)
             assert rc == 0, rc
             launches += 1
         b.record(s)
@@ -119,7 +123,7 @@ class BatchedRunner:
                 resizes += 1
             mx = int(self.sizes[b0:b1].max()) if b1 > b0 else 1
             self.t.apply_batches(self.types, self.keys, self.vals, self.offsets[b0:b1 + 1], max(mx, 1),
-                                 self.status, self.outv, 0, threads_per_block, blocks_per_sm, stream=s)
+                                 self.status, self.outv, self.hints, threads_per_block, blocks_per_sm, stream=s)
         b.record(s)
         torch.cuda.synchronize()
         return RunResult("persistent", a.elapsed_time(b), self.wl.total_ops, len(segs), resizes, segs)

@@ -73,8 +73,9 @@ enum {
 enum : unsigned long long { kErrLockTimeout = 1ull, kErrRetryOut = 2ull };
 
 constexpr uint32_t kFlagHoles = 1u;     // deletes or a resize ran since the last clear
-constexpr uint32_t kFlagUntagged = 2u;  // set on the launch's copy only: this launch leaves the
-                                        // tag words to a rebuild after it (k_retag)
+constexpr uint32_t kFlagUntagged = 2u;  // set on the launch's copy only: the launch neither reads
+                                        // nor keeps the tag words (a bulk insert that rebuilds them
+                                        // after it, or a table too large for them to stay in L2)
 
 // The device view of a table, passed to every kernel by value.
 //
@@ -485,7 +486,11 @@ __device__ __forceinline__ bool find_tagged(const Table& t, uint32_t b, u64 T, u
 // an eviction writes the victim (and its fingerprint) to H1 before removing it from H0, so
 // reading H0 then H1 in that order always finds it.
 template <int P, bool kReadOnly>
+__device__ __forceinline__ bool find_one_buckets(const Table& t, uint32_t k, uint32_t* v);
+
+template <int P, bool kReadOnly>
 __device__ __forceinline__ bool find_one(const Table& t, uint32_t k, uint32_t* v) {
+    if (t.flags & kFlagUntagged) return find_one_buckets<P, kReadOnly>(t, k, v);
     if (k == 0) return false;
     const uint32_t f = tag_of(k);
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
@@ -506,6 +511,33 @@ __device__ __forceinline__ bool find_one(const Table& t, uint32_t k, uint32_t* v
         }
     }
     return false;
+}
+
+// Lookup without tags (a table whose tag words are not kept): H0 whole, then H1, then the stash.
+template <int P, bool kReadOnly>
+__device__ __forceinline__ bool find_one_buckets(const Table& t, uint32_t k, uint32_t* v) {
+    if (k == 0) return false;
+    const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
+    Bucket B;
+    if (kReadOnly) load_bucket_ro(t.slots + (size_t)b0 * kSlots, B);
+    else load_bucket(t.slots + (size_t)b0 * kSlots, B);
+    uint32_t m = match_mask(B, k);
+    if (!m) {
+        const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
+        if (b1 != b0) {
+            if (kReadOnly) load_bucket_ro(t.slots + (size_t)b1 * kSlots, B);
+            else load_bucket(t.slots + (size_t)b1 * kSlots, B);
+            m = match_mask(B, k);
+        }
+        if (!m && (kReadOnly ? stash_flag_ro(t, b0) : stash_flag(t, b0))) {
+            if (kReadOnly) load_bucket_ro(t.stash + (size_t)b0 * kSlots, B);
+            else load_bucket(t.stash + (size_t)b0 * kSlots, B);
+            m = match_mask(B, k);
+        }
+        if (!m) return false;
+    }
+    *v = val_of(slot_at(B, __ffs(m) - 1));
+    return true;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -809,7 +841,7 @@ __device__ __forceinline__ uint8_t claim_or_update_untagged(const Table& t, uint
 // than a 32 B read followed by a CAS that hits.  Returns as claim_or_update_untagged.
 template <bool kTagged = true>
 __device__ __forceinline__ uint8_t claim_or_update(const Table& t, uint32_t b, uint32_t k, u64 kv) {
-    if (!kTagged) return claim_or_update_untagged(t, b, k, kv);
+    if (!kTagged || (t.flags & kFlagUntagged)) return claim_or_update_untagged(t, b, k, kv);
     u64* p = t.slots + (size_t)b * kSlots;
     const uint32_t f = tag_of(k);
     const u64 T = load_tags(t, b);
@@ -849,6 +881,81 @@ __device__ __forceinline__ uint8_t claim_or_update(const Table& t, uint32_t b, u
     return 0;
 }
 
+// With holes and per-slot tags, update k in bucket b if a copy is there.  Only the sectors with
+// a matching fingerprint are read.  A copy that changes key between the read and the CAS was
+// moved by an eviction (its copy is already in H1) and is looked for there.  Returns 1 updated,
+// 0 not in b.
+__device__ __forceinline__ int update_tagged(const Table& t, uint32_t b, uint32_t k, uint32_t f, u64 kv) {
+    u64* p = t.slots + (size_t)b * kSlots;
+    uint32_t m = tag_match(load_tags(t, b), f);
+    while (m) {
+        const int sec = (__ffs(m) - 1) >> 2;
+        m &= ~(0xFu << (4 * sec));
+        Sector S;
+        load_sector(p + 4 * sec, S);
+        const uint32_t hit = sector_match(S, k);
+        if (!hit) continue;
+        u64* sp = p + 4 * sec + (__ffs(hit) - 1);
+        u64 cur = sector_at(S, __ffs(hit) - 1);
+        for (int r = 0; r < kRetryLimit; ++r) {
+            const u64 obs = cas64(sp, cur, kv);
+            if (obs == cur) return 1;
+            if (key_of(obs) != k) break;
+            cur = obs;
+        }
+    }
+    return 0;
+}
+
+// With holes and per-slot tags, claim a free slot of bucket b for kv: the slots whose tag byte is
+// 0, one sector at a time, each sector read before its CAS (a CAS that misses L2 is far slower).
+// Returns kStInserted, or 0 when b has no free slot by its tag word.
+__device__ __forceinline__ uint8_t claim_tagged(const Table& t, uint32_t b, uint32_t f, u64 kv) {
+    u64* p = t.slots + (size_t)b * kSlots;
+    uint32_t e = tag_match(load_tags(t, b), 0u);
+    while (e) {
+        const int sec = (__ffs(e) - 1) >> 2;
+        uint32_t es = (e >> (4 * sec)) & 0xFu;
+        e &= ~(0xFu << (4 * sec));
+        Sector S;
+        load_sector(p + 4 * sec, S);
+        while (es) {
+            const int q = __ffs(es) - 1;
+            es &= es - 1;
+            if (sector_at(S, q) != 0ull) continue;
+            if (cas64(p + 4 * sec + q, 0ull, kv) == 0ull) {
+                tag_set(t, b, 4 * sec + q, f);
+                if (!e && !es) mark_full(t, b);
+                return kStInserted;
+            }
+        }
+    }
+    return 0;
+}
+
+// Lock-free stages A and B with holes, per-slot tags and at most one op per key in the batch: an
+// existing copy is looked for in H0, then H1 (whose tags are read after H0, as in find_one), then
+// the stash; with none, the key claims a free slot of H0, else of H1.  No other insert of the key
+// runs in the batch, so no second copy can appear and there is no duplicate check.  Returns the
+// op's status, or 0 for the locked path.
+template <bool kPrimaryOnly>
+__device__ __noinline__ uint8_t insert_holes_unique(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
+    const uint32_t f = tag_of(k);
+    if (update_tagged(t, b0, k, f, kv)) return kStUpdated;
+    if (b1 != b0 && update_tagged(t, b1, k, f, kv)) return kStUpdated;
+    if (stash_flag(t, b0)) {
+        u64* Sp = t.stash + (size_t)b0 * kSlots;
+        for (int r = 0; r < kRetryLimit; ++r) {
+            const int u = update_in(Sp, k, kv);
+            if (u == 1) return kStUpdated;
+            if (u == 0) break;
+        }
+    }
+    const uint8_t st = claim_tagged(t, b0, f, kv);
+    if (st || b1 == b0 || kPrimaryOnly) return st;
+    return claim_tagged(t, b1, f, kv);
+}
+
 // Which insert protocol a kernel compiles: chosen from the table's flags at run time, or fixed
 // by the host (which knows the flags) so the kernel carries only the code it needs.  The base
 // (low two bits) says whether the table may have holes; two flag bits refine it:
@@ -856,7 +963,10 @@ __device__ __forceinline__ uint8_t claim_or_update(const Table& t, uint32_t b, u
 //                  insert_lockfree)
 //   kModeUntagged  no tag upkeep: a bulk insert whose tag words are rebuilt after it; the
 //                  launch's Table copy carries kFlagUntagged for the code chosen at run time
-enum Mode { kModeRuntime = 0, kModeMono = 1, kModeHoles = 2, kModePrimary = 4, kModeUntagged = 8 };
+//   kModeUnique    the caller guarantees each key at most once in the batch: with holes, an
+//                  insert cannot race another insert of its key, so it finds an existing copy and
+//                  a free slot through the tag words and skips the duplicate check
+enum Mode { kModeRuntime = 0, kModeMono = 1, kModeHoles = 2, kModePrimary = 4, kModeUntagged = 8, kModeUnique = 16 };
 __host__ __device__ constexpr int mode_base(int m) { return m & 3; }
 __device__ __forceinline__ bool tagged(const Table& t) { return !(t.flags & kFlagUntagged); }
 
@@ -879,6 +989,7 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
         if (st || b1 == b0 || kPrimaryOnly) return st;
         return claim_or_update<kTagged>(t, b1, k, kv);
     }
+    if (kTagged && (kMode & kModeUnique) && tagged(t)) return insert_holes_unique<kPrimaryOnly>(t, k, kv, b0, b1);
     // With holes a key may sit in H1 or the stash while H0 has room: scan all three first.
     u64* Sp = t.stash + (size_t)b0 * kSlots;
     for (int r = 0; r < kRetryLimit; ++r) {
@@ -917,6 +1028,7 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
         if (cas64(Cp + j, 0ull, kv) == 0ull) {
             if (kTagged) tag_set(t, cb, j, tag_of(k));
             if (__popc(e) == 1) mark_full(t, cb);
+            if (kMode & kModeUnique) return kStInserted;
             return resolve_duplicate(t, cb, k, j, kv) ? kStUpdated : kStInserted;
         }
     }
@@ -971,7 +1083,7 @@ __device__ __forceinline__ uint8_t insert_deferred_one(const Table& t, uint32_t 
 // full hint is cleared after a removal.
 // A table bucket whose tag word holds no matching fingerprint is not read.
 __device__ __forceinline__ bool erase_in(const Table& t, u64* p, uint32_t k, bool is_slots, uint32_t b) {
-    if (is_slots && !tag_match(load_tags(t, b), tag_of(k))) return false;
+    if (is_slots && tagged(t) && !tag_match(load_tags(t, b), tag_of(k))) return false;
     bool removed = false;
     for (int r = 0; r < kRetryLimit; ++r) {
         Bucket B;

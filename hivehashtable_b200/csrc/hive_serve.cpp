@@ -306,11 +306,13 @@ int hive_serve_run(
         if (rc) break;
         cudaEventRecord(s.staged, s.copy);
         cudaStreamWaitEvent(compute, s.staged, 0);
-        if (s.nf && (rc = hive_apply_ops(t, s.d_ftypes, s.d_fkeys, nullptr, s.nf, s.d_found, s.d_fvals,
-                                         HIVE_HINT_NO_DELETES, compute)))
+        // coalescing leaves each key once per list
+        const uint32_t hints = HIVE_HINT_NO_DELETES | HIVE_HINT_UNIQUE_KEYS;
+        if (s.nf && (rc = hive_apply_ops(t, s.d_ftypes, s.d_fkeys, nullptr, s.nf, s.d_found, s.d_fvals, hints,
+                                         compute)))
             break;
-        if (s.nu && (rc = hive_apply_ops(t, s.d_utypes, s.d_ukeys, s.d_uvals, s.nu, s.d_ust, nullptr,
-                                         HIVE_HINT_NO_DELETES, compute)))
+        if (s.nu && (rc = hive_apply_ops(t, s.d_utypes, s.d_ukeys, s.d_uvals, s.nu, s.d_ust, nullptr, hints,
+                                         compute)))
             break;
         cudaEventRecord(s.done, compute);
         cudaStreamWaitEvent(s.copy, s.done, 0);

@@ -75,7 +75,10 @@ struct hive_table {
     void* rbuf = nullptr;         // region-ordering buffers (13 bytes per op of the largest batch)
     uint64_t rcap = 0;
     int num_sms = 148;
-    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1};  // HIVE_TUNE_* knobs
+    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1, 1};  // HIVE_TUNE_* knobs
+    bool tags_valid = true;  // the tag words match the slots (a zeroed table's do)
+    void* ovf = nullptr;     // shrink: overflow entries of one merge step (kept between calls)
+    size_t ovf_cap = 0;      // entries
     // host-buffer pipeline (hive_insert_host / hive_find_host): copy streams, events and device
     // staging arrays (insert keys, values, statuses; find keys, values, flags: 18 bytes per op)
     cudaStream_t pipe_h2d = nullptr, pipe_d2h = nullptr;
@@ -583,16 +586,17 @@ __global__ void k_verify(hive::Table t, uint64_t nb, bool strict, u64* out) {
     hive::Bucket B;
     hive::load_bucket_ro(t.slots + b * hive::kSlots, B);
     const u64 T = t.tags[b];
+    const bool tags = !(t.flags & hive::kFlagUntagged);  // a table without tags: no tag checks
     u64 bad[HIVE_VERIFY_COUNT] = {0, 0, 0, 0};
     for (int j = 0; j < hive::kSlots; ++j) {
         const u64 kv = B.s[j];
         const uint32_t byte = (uint32_t)(T >> (8 * j)) & 0xFFu;
         if (!kv) {
-            bad[HIVE_VERIFY_STALE_TAG] += strict && byte != 0;
+            bad[HIVE_VERIFY_STALE_TAG] += tags && strict && byte != 0;
             continue;
         }
         const uint32_t k = hive::key_of(kv);
-        bad[HIVE_VERIFY_TAG_MISMATCH] += byte != hive::tag_of(k);
+        bad[HIVE_VERIFY_TAG_MISMATCH] += tags && byte != hive::tag_of(k);
         bad[HIVE_VERIFY_MISPLACED] +=
             hive::bucket_addr(t, hive::Policy<P>::h0(k)) != b && hive::bucket_addr(t, hive::Policy<P>::h1(k)) != b;
         for (int q = 0; q < j; ++q) bad[HIVE_VERIFY_DUPLICATE] += hive::key_of(B.s[q]) == k;
@@ -773,6 +777,41 @@ int reset(hive_table* h, cudaStream_t s) {
 
 bool valid_table(const hive_table* h) { return h && h->block; }
 
+// Per-slot tags pay while their words stay in L2 (8 bytes per bucket).  Beyond that a tag word
+// is one more random DRAM access per op, so larger tables run without them (HIVE_TUNE_TAGS:
+// 0 never, 1 while the words fit kTagL2Bytes, 2 always).
+constexpr uint64_t kTagL2Bytes = 64ull << 20;
+bool use_tags(const hive_table* h) {
+    const int64_t m = h->tune[HIVE_TUNE_TAGS];
+    return m == 2 || (m == 1 && num_buckets(h) * 8 <= kTagL2Bytes);
+}
+
+hive::Table untagged_view(const hive_table* h) {
+    hive::Table t = h->t;
+    t.flags |= hive::kFlagUntagged;
+    return t;
+}
+
+// Rebuild the tag words of the buckets in use from their slots.
+void retag(hive_table* h, cudaStream_t s) {
+    const uint64_t nb = num_buckets(h);
+    k_retag<<<grid_for(nb), kBlock, 0, s>>>(h->t, nb);
+    h->tags_valid = true;
+}
+
+// The Table copy a launch uses: with tags when the table uses them (rebuilding stale words first),
+// else marked untagged, which leaves the words stale.
+int table_view(hive_table* h, cudaStream_t s, hive::Table* tv) {
+    if (use_tags(h)) {
+        if (!h->tags_valid) retag(h, s);
+        *tv = h->t;
+    } else {
+        *tv = untagged_view(h);
+        h->tags_valid = false;
+    }
+    return launch_check();
+}
+
 // The deferred-op queue for a batch of n ops; grows (synchronously) to the largest batch seen.
 // Batches of 2^32 ops or more run without deferral.
 int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d) {
@@ -920,6 +959,10 @@ int split_range(hive_table* h, uint32_t cnt, cudaStream_t s) {
     return HIVE_OK;
 }
 
+// Buckets folded per merge step: bounds the overflow buffer (16 entries per folded bucket: its 8
+// slots and 8 stash entries) at 128 MiB, allocated once and kept by the table.
+constexpr uint32_t kMergeStep = 1u << 20;
+
 template <int P>
 int merge_range(hive_table* h, uint32_t cnt, cudaStream_t s) {
     // Fold buckets [split - cnt, split) + n_lo back into [split - cnt, split).
@@ -927,9 +970,17 @@ int merge_range(hive_table* h, uint32_t cnt, cudaStream_t s) {
     const uint32_t lo = h->t.split - cnt;
     hive::Table tnew = told;
     tnew.split = lo;
-    u64* ovf = nullptr;
     const size_t ovf_cap = (size_t)cnt * 16 + 1;
-    HIVE_CUDA(cudaMallocAsync(&ovf, ovf_cap * 8 + 16, s));
+    if (ovf_cap > h->ovf_cap) {
+        HIVE_CUDA(cudaStreamSynchronize(s));
+        if (h->ovf) cudaFree(h->ovf);
+        h->ovf = nullptr;
+        h->ovf_cap = 0;
+        cudaError_t e = cudaMalloc(&h->ovf, ovf_cap * 8 + 16);
+        if (e != cudaSuccess) return cuda_fail(e);
+        h->ovf_cap = ovf_cap;
+    }
+    u64* ovf = (u64*)h->ovf;
     u64* novf = ovf + ovf_cap;
     uint8_t* fail = (uint8_t*)(novf + 1);
     HIVE_CUDA(cudaMemsetAsync(novf, 0, 16, s));
@@ -938,11 +989,11 @@ int merge_range(hive_table* h, uint32_t cnt, cudaStream_t s) {
     if (rc) return rc;
     h->t.split = lo;
     tnew.flags |= hive::kFlagHoles;
+    if (!h->tags_valid) tnew.flags |= hive::kFlagUntagged;  // stale words are neither read nor kept
     k_reinsert<P><<<(unsigned)((ovf_cap + 255) / 256), 256, 0, s>>>(tnew, ovf, novf, fail);
     if ((rc = launch_check())) return rc;
     uint8_t hfail = 0;
     HIVE_CUDA(cudaMemcpyAsync(&hfail, fail, 1, cudaMemcpyDeviceToHost, s));
-    HIVE_CUDA(cudaFreeAsync(ovf, s));
     HIVE_CUDA(cudaStreamSynchronize(s));
     return hfail ? HIVE_ERR_CAPACITY : HIVE_OK;
 }
@@ -962,7 +1013,7 @@ int resize_impl(hive_table* h, uint64_t target_buckets, cudaStream_t s) {
             set_geometry(h, h->level - 1, h->t.n_lo >> 1);
         }
         const uint64_t extra = num_buckets(h) - target_buckets;
-        const uint32_t cnt = (uint32_t)std::min<uint64_t>(extra, h->t.split);
+        const uint32_t cnt = (uint32_t)std::min<uint64_t>(std::min<uint64_t>(extra, h->t.split), kMergeStep);
         if ((rc = merge_range<P>(h, cnt, s))) return rc;
     }
     return HIVE_OK;
@@ -1050,6 +1101,7 @@ int hive_destroy(hive_table* h) {
         if (h->defer_q && (e = cudaFree(h->defer_q)) != cudaSuccess) rc = cuda_fail(e);
         if (h->rbuf && (e = cudaFree(h->rbuf)) != cudaSuccess) rc = cuda_fail(e);
         if (h->hbuf && (e = cudaFree(h->hbuf)) != cudaSuccess) rc = cuda_fail(e);
+        if (h->ovf && (e = cudaFree(h->ovf)) != cudaSuccess) rc = cuda_fail(e);
         for (cudaEvent_t ev : {h->ev_in, h->ev_out, h->ev_ins_free, h->ev_find_free})
             if (ev) cudaEventDestroy(ev);
         for (cudaStream_t st : {h->pipe_h2d, h->pipe_d2h})
@@ -1067,6 +1119,7 @@ int hive_clear(hive_table* h, void* stream) {
     if (rc) return rc;
     set_geometry(h, 0, 0);
     h->t.flags = 0;
+    h->tags_valid = true;  // zeroed words describe the empty table
     return HIVE_OK;
 }
 
@@ -1077,7 +1130,9 @@ int hive_clear(hive_table* h, void* stream) {
     } while (0)
 
 // Launch a two-pass kernel: the first pass with deferral when the queue exists, else one pass.
-#define HIVE_DISPATCH_D(kern, d, grid, block, stream, ...)                                  \
+// HIVE_DISPATCH_DX adds the mode bits `extra` to the holes and run-time modes (kModeUnique).
+#define HIVE_DISPATCH_D(kern, d, grid, block, stream, ...) HIVE_DISPATCH_DX(kern, 0, d, grid, block, stream, __VA_ARGS__)
+#define HIVE_DISPATCH_DX(kern, extra, d, grid, block, stream, ...)                          \
     do {                                                                                   \
         const bool p1_ = h->policy == HIVE_POLICY_MURMURCITYHASH;                          \
         const bool holes_ = h->t.flags & hive::kFlagHoles;                                 \
@@ -1085,11 +1140,11 @@ int hive_clear(hive_table* h, void* stream) {
             if (p1_) kern<1, true, hive::kModeMono><<<grid, block, 0, stream>>>(__VA_ARGS__);  \
             else kern<0, true, hive::kModeMono><<<grid, block, 0, stream>>>(__VA_ARGS__);      \
         } else if (d.q) {                                                                  \
-            if (p1_) kern<1, true, hive::kModeHoles><<<grid, block, 0, stream>>>(__VA_ARGS__); \
-            else kern<0, true, hive::kModeHoles><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
+            if (p1_) kern<1, true, hive::kModeHoles | (extra)><<<grid, block, 0, stream>>>(__VA_ARGS__); \
+            else kern<0, true, hive::kModeHoles | (extra)><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
         } else {                                                                           \
-            if (p1_) kern<1, false, hive::kModeRuntime><<<grid, block, 0, stream>>>(__VA_ARGS__); \
-            else kern<0, false, hive::kModeRuntime><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
+            if (p1_) kern<1, false, hive::kModeRuntime | (extra)><<<grid, block, 0, stream>>>(__VA_ARGS__); \
+            else kern<0, false, hive::kModeRuntime | (extra)><<<grid, block, 0, stream>>>(__VA_ARGS__);     \
         }                                                                                  \
     } while (0)
 
@@ -1106,11 +1161,21 @@ bool bulk_untagged(const hive_table* h, uint64_t n) {
     return m == 2 || (m == 1 && n * 8 >= num_buckets(h));
 }
 
-// The Table copy a bulk insert launches with.
-hive::Table insert_view(const hive_table* h, bool untagged) {
-    hive::Table t = h->t;
-    if (untagged) t.flags |= hive::kFlagUntagged;
-    return t;
+// The Table copy an insert of n ops launches with, and whether the tag words must be rebuilt
+// after it (*retag_after).  Without tags (use_tags false) nothing reads or keeps them.
+int insert_view(hive_table* h, uint64_t n, cudaStream_t s, hive::Table* tv, bool* retag_after) {
+    *retag_after = false;
+    if (!use_tags(h)) {
+        *tv = untagged_view(h);
+        h->tags_valid = false;
+        return HIVE_OK;
+    }
+    if (bulk_untagged(h, n)) {
+        *tv = untagged_view(h);
+        *retag_after = true;
+        return HIVE_OK;
+    }
+    return table_view(h, s, tv);
 }
 
 // First pass of an insert (k_insert) over ops [lo, hi): deferring when the queue exists, with
@@ -1145,11 +1210,6 @@ void launch_first_pass(const hive_table* h, const hive::Table& t, const Defer& d
     }
 }
 
-// Rebuild the tag words of the buckets in use from their slots (after an untagged bulk insert).
-void retag(const hive_table* h, cudaStream_t s) {
-    const uint64_t nb = num_buckets(h);
-    k_retag<<<grid_for(nb), kBlock, 0, s>>>(h->t, nb);
-}
 
 }  // namespace
 
@@ -1165,8 +1225,9 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
     Defer d;
     int rc = prepare_defer(h, n, s, &d);
     if (rc) return rc;
-    const bool untag = bulk_untagged(h, n);
-    const hive::Table tt = insert_view(h, untag);
+    hive::Table tt;
+    bool untag;
+    if ((rc = insert_view(h, n, s, &tt, &untag))) return rc;
     if (use_regions(h, n, HIVE_TUNE_REGION_INSERT)) {
         // region-ordered: sort, both passes over the sorted arrays, statuses back to caller order
         Regions r;
@@ -1241,8 +1302,9 @@ int hive_insert_noalloc(hive_table* h, const uint32_t* keys, const uint32_t* val
     cudaStream_t s = (cudaStream_t)stream;
     Defer d{base + kNoAllocHeaderWords, (u64*)base};
     HIVE_CUDA(cudaMemsetAsync(d.n, 0, sizeof(u64), s));  // the queue count must start at zero
-    const bool untag = bulk_untagged(h, n);
-    const hive::Table tt = insert_view(h, untag);
+    hive::Table tt;
+    bool untag;
+    if ((rc = insert_view(h, n, s, &tt, &untag))) return rc;
     launch_first_pass(h, tt, d, 0, n, s, keys, values, status, false);
     HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, tt, keys, values, status, d);
     if (untag) retag(h, s);
@@ -1255,15 +1317,17 @@ int hive_find(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* values,
     if (!keys) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
+    hive::Table tv;
+    if (int vrc = table_view(h, s, &tv)) return vrc;
     if (use_regions(h, n, HIVE_TUNE_REGION_FIND)) {
         Regions r;
         int rc;
         if ((rc = prepare_regions(h, n, 1, s, &r)) || (rc = region_sort(h, keys, nullptr, n, r, s))) return rc;
-        HIVE_DISPATCH(k_find, grid_for(n), kBlock, s, h->t, r.rkeys, n, r.rvals, r.rst);
+        HIVE_DISPATCH(k_find, grid_for(n), kBlock, s, tv, r.rkeys, n, r.rvals, r.rst);
         k_unpermute_find<<<grid_for(n), kBlock, 0, s>>>(r.ridx, r.rvals, r.rst, n, values, found);
         return launch_check();
     }
-    HIVE_DISPATCH(k_find, grid_for(n), kBlock, s, h->t, keys, n, values, found);
+    HIVE_DISPATCH(k_find, grid_for(n), kBlock, s, tv, keys, n, values, found);
     return launch_check();
 }
 
@@ -1334,8 +1398,9 @@ int hive_insert_host(hive_table* h, const uint32_t* keys, const uint32_t* values
     if ((rc = prepare_pipe(h, n, &st)) || (rc = prepare_defer(h, n, s, &d))) return rc;
     HIVE_CUDA(cudaStreamWaitEvent(h->pipe_h2d, h->ev_ins_free, 0));
     uint8_t* dst = status ? st.ist : nullptr;
-    const bool untag = bulk_untagged(h, n);
-    const hive::Table tt = insert_view(h, untag);
+    hive::Table tt;
+    bool untag;
+    if ((rc = insert_view(h, n, s, &tt, &untag))) return rc;
     for (uint64_t lo = 0; lo < n; lo += kPipeChunk) {
         const uint64_t m = std::min(kPipeChunk, n - lo);
         HIVE_CUDA(cudaMemcpyAsync(st.ik + lo, keys + lo, m * 4, cudaMemcpyHostToDevice, h->pipe_h2d));
@@ -1365,12 +1430,14 @@ int hive_find_host(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* va
     Staging st;
     int rc = prepare_pipe(h, n, &st);
     if (rc) return rc;
+    hive::Table tv;
+    if (int vrc = table_view(h, s, &tv)) return vrc;
     HIVE_CUDA(cudaStreamWaitEvent(h->pipe_h2d, h->ev_find_free, 0));
     for (uint64_t lo = 0; lo < n; lo += kPipeChunk) {
         const uint64_t m = std::min(kPipeChunk, n - lo);
         HIVE_CUDA(cudaMemcpyAsync(st.fk + lo, keys + lo, m * 4, cudaMemcpyHostToDevice, h->pipe_h2d));
         HIVE_CUDA(order(h->ev_in, h->pipe_h2d, s));
-        HIVE_DISPATCH(k_find, grid_for(m), kBlock, s, h->t, st.fk + lo, m, st.fv + lo, st.ff + lo);
+        HIVE_DISPATCH(k_find, grid_for(m), kBlock, s, tv, st.fk + lo, m, st.fv + lo, st.ff + lo);
         if (values || found) HIVE_CUDA(order(h->ev_out, s, h->pipe_d2h));
         if (values) HIVE_CUDA(cudaMemcpyAsync(values + lo, st.fv + lo, m * 4, cudaMemcpyDeviceToHost, h->pipe_d2h));
         if (found) HIVE_CUDA(cudaMemcpyAsync(found + lo, st.ff + lo, m, cudaMemcpyDeviceToHost, h->pipe_d2h));
@@ -1386,7 +1453,10 @@ int hive_erase(hive_table* h, const uint32_t* keys, uint64_t n, uint8_t* status,
     if (!keys) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     h->t.flags |= hive::kFlagHoles;
-    HIVE_DISPATCH(k_erase, grid_for(n), kBlock, (cudaStream_t)stream, h->t, keys, n, status);
+    cudaStream_t s = (cudaStream_t)stream;
+    hive::Table tv;
+    if (int vrc = table_view(h, s, &tv)) return vrc;
+    HIVE_DISPATCH(k_erase, grid_for(n), kBlock, s, tv, keys, n, status);
     return launch_check();
 }
 
@@ -1401,9 +1471,15 @@ int hive_apply_ops(hive_table* h, const uint8_t* types, const uint32_t* keys, co
     Defer d;
     int rc = prepare_defer(h, n, s, &d);
     if (rc) return rc;
-    HIVE_DISPATCH_D(k_apply, d, grid_for(n), kBlock, s, h->t, types, keys, values, n, status, out_values, d);
+    hive::Table tv;
+    if (int vrc = table_view(h, s, &tv)) return vrc;
+    if (hints & HIVE_HINT_UNIQUE_KEYS)
+        HIVE_DISPATCH_DX(k_apply, hive::kModeUnique, d, grid_for(n), kBlock, s, tv, types, keys, values, n, status,
+                         out_values, d);
+    else
+        HIVE_DISPATCH_D(k_apply, d, grid_for(n), kBlock, s, tv, types, keys, values, n, status, out_values, d);
     if (d.q)
-        HIVE_DISPATCH(k_apply_deferred, second_pass_grid(h, n), kBlock, s, h->t, keys, values, status, out_values, d);
+        HIVE_DISPATCH(k_apply_deferred, second_pass_grid(h, n), kBlock, s, tv, keys, values, status, out_values, d);
     return launch_check();
 }
 
@@ -1422,19 +1498,22 @@ int hive_apply_batches(hive_table* h, const uint8_t* types, const uint32_t* keys
     int rc = prepare_defer(h, max_batch_ops, s, &d);
     if (rc) return rc;
     if (!d.q) return HIVE_ERR_INVALID_ARG;
+    hive::Table tv;
+    if (int vrc = table_view(h, s, &tv)) return vrc;
     HIVE_CUDA(cudaMemsetAsync(h->scratch, 0, 16, s));  // both alternating queue counts
     const bool holes = h->t.flags & hive::kFlagHoles;
     const bool p1 = h->policy == HIVE_POLICY_MURMURCITYHASH;
-    const void* fn = p1 ? (holes ? (const void*)k_apply_batches<1, hive::kModeHoles>
+    const bool uniq = hints & HIVE_HINT_UNIQUE_KEYS;
+    constexpr int kHU = hive::kModeHoles | hive::kModeUnique;
+    const void* fn = p1 ? (holes ? (uniq ? (const void*)k_apply_batches<1, kHU> : (const void*)k_apply_batches<1, hive::kModeHoles>)
                                  : (const void*)k_apply_batches<1, hive::kModeMono>)
-                        : (holes ? (const void*)k_apply_batches<0, hive::kModeHoles>
+                        : (holes ? (uniq ? (const void*)k_apply_batches<0, kHU> : (const void*)k_apply_batches<0, hive::kModeHoles>)
                                  : (const void*)k_apply_batches<0, hive::kModeMono>);
     int fit = 0;
     HIVE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, threads_per_block, 0));
     if (fit < 1) return HIVE_ERR_INVALID_ARG;
     const int per_sm = blocks_per_sm > 0 ? std::min(blocks_per_sm, fit) : fit;
     dim3 grid((unsigned)(per_sm * h->num_sms)), block((unsigned)threads_per_block);
-    hive::Table tv = h->t;
     u64* qn = h->scratch;  // two counts: scratch[0], scratch[1]
     void* args[] = {(void*)&tv, (void*)&types, (void*)&keys, (void*)&values, (void*)&offsets, (void*)&n_batches,
                     (void*)&status, (void*)&out_values, (void*)&d.q, (void*)&qn};
@@ -1448,20 +1527,27 @@ int hive_apply_reference_ops(hive_table* h, const void* ops, uint64_t n, uint64_
     if (n == 0) return HIVE_OK;
     if (!ops || ((uintptr_t)ops & 15)) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    // the holes flag first: the launch's view carries the flags
+    if (!(hints & (HIVE_HINT_LOOKUPS_ONLY | HIVE_HINT_NO_DELETES))) h->t.flags |= hive::kFlagHoles;
+    hive::Table tv;
+    if (int vrc = table_view(h, s, &tv)) return vrc;
     if (hints & HIVE_HINT_LOOKUPS_ONLY) {
-        HIVE_DISPATCH(k_apply_ref_ro, grid_for(n), kBlock, (cudaStream_t)stream, h->t, (const ulonglong2*)ops, n,
+        HIVE_DISPATCH(k_apply_ref_ro, grid_for(n), kBlock, s, tv, (const ulonglong2*)ops, n,
                       (unsigned long long*)results);
         return launch_check();
     }
-    cudaStream_t s = (cudaStream_t)stream;
-    if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
     Defer d;
     int rc = prepare_defer(h, n, s, &d);
     if (rc) return rc;
-    HIVE_DISPATCH_D(k_apply_ref, d, grid_for(n), kBlock, s, h->t, (const ulonglong2*)ops, n,
-                    (unsigned long long*)results, d);
+    if (hints & HIVE_HINT_UNIQUE_KEYS)
+        HIVE_DISPATCH_DX(k_apply_ref, hive::kModeUnique, d, grid_for(n), kBlock, s, tv, (const ulonglong2*)ops, n,
+                         (unsigned long long*)results, d);
+    else
+        HIVE_DISPATCH_D(k_apply_ref, d, grid_for(n), kBlock, s, tv, (const ulonglong2*)ops, n,
+                        (unsigned long long*)results, d);
     if (d.q)
-        HIVE_DISPATCH(k_apply_ref_deferred, second_pass_grid(h, n), kBlock, s, h->t, (const ulonglong2*)ops,
+        HIVE_DISPATCH(k_apply_ref_deferred, second_pass_grid(h, n), kBlock, s, tv, (const ulonglong2*)ops,
                       (unsigned long long*)results, d);
     return launch_check();
 }
@@ -1565,10 +1651,12 @@ int hive_verify(hive_table* h, uint64_t* out, void* stream) {
     DeviceGuard g(h->device);
     if (!g.ok) return HIVE_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
+    hive::Table tv;
+    if (int vrc = table_view(h, s, &tv)) return vrc;
     u64* d = h->scratch + 2;  // scratch words 2..5
     HIVE_CUDA(cudaMemsetAsync(d, 0, HIVE_VERIFY_COUNT * 8, s));
     const uint64_t nb = num_buckets(h);
-    HIVE_DISPATCH(k_verify, grid_for(nb), kBlock, s, h->t, nb, !(h->t.flags & hive::kFlagHoles), d);
+    HIVE_DISPATCH(k_verify, grid_for(nb), kBlock, s, tv, nb, !(h->t.flags & hive::kFlagHoles), d);
     int rc = launch_check();
     if (rc) return rc;
     HIVE_CUDA(cudaMemcpyAsync(out, d, HIVE_VERIFY_COUNT * 8, cudaMemcpyDeviceToHost, s));
@@ -1578,7 +1666,7 @@ int hive_verify(hive_table* h, uint64_t* out, void* stream) {
 
 int hive_set_tuning(hive_table* h, int32_t key, int64_t value) {
     if (!valid_table(h) || key < 0 || key >= HIVE_NUM_TUNES) return HIVE_ERR_INVALID_ARG;
-    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0}, hi[HIVE_NUM_TUNES] = {1, 1, 8, 8, 2};
+    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0, 0}, hi[HIVE_NUM_TUNES] = {1, 1, 8, 8, 2, 2};
     if (value < lo[key] || value > hi[key]) return HIVE_ERR_INVALID_ARG;
     h->tune[key] = value;
     return HIVE_OK;

@@ -33,11 +33,14 @@ ERRORS = {
 ST_FAIL, ST_INSERTED, ST_UPDATED, ST_STASHED, ST_ERROR = 0, 1, 2, 3, 255
 OP_INSERT, OP_LOOKUP, OP_DELETE, OP_INCREMENT, OP_NONE = 0, 1, 2, 3, 4
 HINT_NO_DELETES = 1
+HINT_LOOKUPS_ONLY = 2
+HINT_UNIQUE_KEYS = 4
 NUM_COUNTERS = 16
 COUNTER_NAMES = {0: "slow_path", 1: "evictions", 2: "stash_push", 3: "failed", 4: "lock_timeout",
                  5: "retry_out", 6: "dup_fixed", 15: "error_bits"}
 # Launch-tuning knobs (HIVE_TUNE_*): how a batch runs, never what it computes
-TUNES = {"region_insert": 0, "region_find": 1, "subbatches": 2, "second_pass_blocks": 3, "bulk_retag": 4}
+TUNES = {"region_insert": 0, "region_find": 1, "subbatches": 2, "second_pass_blocks": 3, "bulk_retag": 4,
+         "tags": 5}
 
 # Policy names accepted by the reference's dispatcher (src/hive_dispatch.cu:829-871).  The
 # ones outside the hot path fall back to Default2Hash with a message, as the reference does for

@@ -62,6 +62,12 @@ extern "C" {
 #define HIVE_HINT_LOOKUPS_ONLY 2u /* batch holds only LOOKUP/NONE ops and no other call modifies the
                                      table meanwhile: lookups take the read-only load path and any
                                      other op type is answered 0 without running               */
+#define HIVE_HINT_UNIQUE_KEYS 4u  /* caller guarantees each key appears at most once in the batch
+                                     (as a coalescing server or a deduplicated batch does): on a
+                                     table that has had deletes, inserts then find an existing
+                                     copy and a free slot from the per-slot fingerprints and skip
+                                     the check for a racing second insert of their key.  A batch
+                                     that breaks the promise may keep two copies of a key    */
 
 /* ---- counters (hive_counters) ---------------------------------------------------------------- */
 #define HIVE_CTR_SLOW_PATH 0    /* inserts whose canonical bucket was full                     */
@@ -264,7 +270,11 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
                                         (default) per op for batches under one op per eight
                                         buckets, else one rebuild of the fingerprints after the
                                         batch; 2 always the rebuild                              */
-#define HIVE_NUM_TUNES 5
+#define HIVE_TUNE_TAGS 5             /* per-slot fingerprints: 0 never (lookups read whole buckets);
+                                        1 (default) while their words (8 bytes per bucket) fit
+                                        64 MiB, i.e. up to 2^23 buckets, where they stay in L2;
+                                        2 always                                                */
+#define HIVE_NUM_TUNES 6
 
 /* Set knob `key` to `value`.  HIVE_ERR_INVALID_ARG for an unknown key or a value out of range. */
 int hive_set_tuning(hive_table* t, int32_t key, int64_t value);

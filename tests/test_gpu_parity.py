@@ -10,8 +10,8 @@ import pytest
 import torch
 
 import oracle
-from hivehashtable_b200 import (OP_DELETE, OP_INCREMENT, OP_INSERT, OP_LOOKUP, OP_NONE, ST_ERROR, ST_FAIL, HiveError,
-                                ST_INSERTED, ST_STASHED, ST_UPDATED, HiveHashTable, u32)
+from hivehashtable_b200 import (HINT_UNIQUE_KEYS, OP_DELETE, OP_INCREMENT, OP_INSERT, OP_LOOKUP, OP_NONE, ST_ERROR,
+                                ST_FAIL, HiveError, ST_INSERTED, ST_STASHED, ST_UPDATED, HiveHashTable, u32)
 from hivehashtable_b200 import workload
 
 pytestmark = pytest.mark.gpu
@@ -210,11 +210,50 @@ def test_tag_upkeep_modes(cuda, policy, retag):
         t.check()
 
 
+@pytest.mark.parametrize("policy", POLICIES)
+def test_tags_switched_off_and_on(cuda, policy):
+    """Fingerprints off (HIVE_TUNE_TAGS 0, as for tables too large for their tag words to stay in
+    L2), then on again: lookups read whole buckets while off, the stale tag words are rebuilt on
+    the first launch after they are switched on, and results equal the replay throughout."""
+    cap = 1 << 18
+    keys, absent, st = oracle.gen_keys(31, int(0.9 * cap), 1 << 14)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    third = keys.size // 3
+    with HiveHashTable(cap, policy) as t:
+        t.set_tuning(tags=0)
+        _insert_and_check(t, m, keys[:third], vals[:third])
+        look, st = oracle.lookup_set(keys[:third], absent, 1 << 13, 1 << 13, st)
+        _find_and_check(t, m, look)
+        gone = keys[: third // 4].copy()
+        np.testing.assert_array_equal(_np(t.erase(gone)), m.erase(gone))
+        _assert_same_set(t, m)
+        t.set_tuning(tags=2)
+        small = keys[third: third + 2000].copy()  # a small batch: per-op fingerprint upkeep
+        _insert_and_check(t, m, small, oracle.values_for(small))
+        _find_and_check(t, m, np.concatenate([look, small]))
+        _assert_same_set(t, m)
+        t.set_tuning(tags=0)
+        _insert_and_check(t, m, keys[third + 2000:], vals[third + 2000:])
+        t.set_tuning(tags=2)
+        look, st = oracle.lookup_set(keys, absent, 1 << 14, 1 << 14, st)
+        _find_and_check(t, m, look)
+        types = np.where(np.arange(look.size) % 3 == 0, OP_INSERT, OP_LOOKUP).astype(np.uint8)
+        uk, ui = np.unique(look, return_index=True)
+        st_a, ov_a = t.apply(types[ui], uk, oracle.values_for(uk) ^ np.uint32(7), hints=HINT_UNIQUE_KEYS)
+        est, eov = m.apply(types[ui], uk, oracle.values_for(uk) ^ np.uint32(7))
+        np.testing.assert_array_equal(np.where(_np(st_a) == ST_STASHED, 1, _np(st_a)), est)
+        np.testing.assert_array_equal(u32(ov_a), eov)
+        _assert_same_set(t, m)
+        t.check()
+
+
 def test_tuning_bounds(cuda):
     with HiveHashTable(1 << 12) as t:
         assert t.tuning() == {"region_insert": 0, "region_find": 0, "subbatches": 0, "second_pass_blocks": 4,
-                              "bulk_retag": 1}
-        for bad in ({"region_insert": 2}, {"subbatches": 9}, {"second_pass_blocks": 0}, {"bulk_retag": 3}):
+                              "bulk_retag": 1, "tags": 1}
+        for bad in ({"region_insert": 2}, {"subbatches": 9}, {"second_pass_blocks": 0}, {"bulk_retag": 3},
+                    {"tags": 3}):
             with pytest.raises(HiveError):
                 t.set_tuning(**bad)
         t.set_tuning(second_pass_blocks=8)
@@ -274,9 +313,11 @@ def test_erase_then_reinsert(cuda, policy):
 
 
 @pytest.mark.parametrize("policy", POLICIES)
-def test_mixed_batches(cuda, policy):
-    """Batches of 50 % insert (new keys), 40 % lookup (80 % present), 10 % delete (present keys,
-    disjoint from the lookups); at most one op per key per batch, so every op's result is fixed."""
+@pytest.mark.parametrize("hints", [0, HINT_UNIQUE_KEYS])
+def test_mixed_batches(cuda, policy, hints):
+    """Batches of 50 % insert (new keys), 10 % upsert of live keys, 30 % lookup (80 % present),
+    10 % delete (live keys); at most one op per key per batch, so every op's result is fixed and
+    the unique-keys hint holds."""
     rng_state = 11
     pre, pool, rng_state = oracle.gen_keys(rng_state, 60_000, 400_000)
     m = oracle.ReplayMap()
@@ -287,21 +328,24 @@ def test_mixed_batches(cuda, policy):
         rs = np.random.RandomState(5)
         for b in range(12):
             size = int(2 ** rs.uniform(10, 15))
-            ni, nl, nd = size // 2, size * 4 // 10, size - size // 2 - size * 4 // 10
+            ni, nu, nl = size // 2, size // 10, size * 3 // 10
+            nd = size - ni - nu - nl
             new = pool[pool_i: pool_i + ni]
             pool_i += ni
             livea = np.array(live, dtype=np.uint32)
-            sel = rs.choice(livea.size, size=nl + nd, replace=False)
-            lk_present = livea[sel[: int(nl * 0.8)]]
+            sel = rs.choice(livea.size, size=nu + nl + nd, replace=False)
+            upd = livea[sel[:nu]]
+            lk_present = livea[sel[nu: nu + int(nl * 0.8)]]
             lk_absent = pool[pool_i: pool_i + (nl - lk_present.size)]
             pool_i += lk_absent.size
-            dels = livea[sel[nl: nl + nd]]
-            keys = np.concatenate([new, lk_present, lk_absent, dels]).astype(np.uint32)
-            types = np.concatenate([np.full(ni, OP_INSERT), np.full(nl, OP_LOOKUP), np.full(nd, OP_DELETE)]).astype(np.uint8)
-            vals = oracle.values_for(keys)
+            dels = livea[sel[nu + nl: nu + nl + nd]]
+            keys = np.concatenate([new, upd, lk_present, lk_absent, dels]).astype(np.uint32)
+            types = np.concatenate([np.full(ni + nu, OP_INSERT), np.full(nl, OP_LOOKUP),
+                                    np.full(nd, OP_DELETE)]).astype(np.uint8)
+            vals = oracle.values_for(keys) ^ np.uint32(b)
             perm = rs.permutation(keys.size)
             keys, types, vals = keys[perm], types[perm], vals[perm]
-            st, ov = t.apply(types, keys, vals)
+            st, ov = t.apply(types, keys, vals, hints=hints)
             st, ov = _np(st), u32(ov)
             assert not (st == ST_ERROR).any()
             ok_ins = (types != OP_INSERT) | (st != ST_FAIL)
