@@ -151,7 +151,8 @@ def random_bucket_ceiling(dev, table_bytes):
              ("read32_table", table_bytes, 3, 32), ("read64_cas_table", table_bytes, 1, 96),
              ("cas_only_table", table_bytes, 5, 32), ("read32_cas_table", table_bytes, 6, 64),
              ("read64x2_table", table_bytes, 2, 128), ("read64x2_indep_table", table_bytes, 4, 128),
-             ("read64_32MiB_l2", 32 << 20, 0, 64)]
+             ("read64_32MiB_l2", 32 << 20, 0, 64), ("read64_cas_32MiB_l2", 32 << 20, 1, 96),
+             ("cas_only_32MiB_l2", 32 << 20, 5, 32)]
     for name, size, mode, bpo in cases:
         buf = torch.zeros(size // 8, dtype=torch.int64, device=dev)
         nb = size // 64

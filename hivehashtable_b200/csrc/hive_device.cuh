@@ -73,6 +73,9 @@ enum {
 enum : unsigned long long { kErrLockTimeout = 1ull, kErrRetryOut = 2ull };
 
 constexpr uint32_t kFlagHoles = 1u;     // deletes or a resize ran since the last clear
+constexpr uint32_t kFlagEvictH1 = 4u;   // set on the launch's copy only: the locked path tries
+                                        // H1's own keys as victims before the stash (region-
+                                        // ordered batches), not only once the stash is full
 constexpr uint32_t kFlagUntagged = 2u;  // set on the launch's copy only: the launch neither reads
                                         // nor keeps the tag words (a bulk insert that rebuilds them
                                         // after it, or a table too large for them to stay in L2)
@@ -325,6 +328,16 @@ __device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
     return false;
 }
 __device__ __forceinline__ void unlock_bucket(const Table& t, uint32_t b) { atomicExch(t.locks + b, 0u); }
+
+// A few attempts at the lock of a second bucket while the first one is held: never waits long,
+// so two evictors that each hold one of the pair and want the other cannot block each other.
+__device__ __forceinline__ bool try_lock_bucket(const Table& t, uint32_t b) {
+    for (int i = 0; i < 4; ++i) {
+        if (atomicCAS(t.locks + b, 0u, 1u) == 0u) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
 
 // ---------------------------------------------------------------------------------------------
 // Slot tags (see the layout above)
@@ -715,6 +728,16 @@ __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket&
     return kEvNone;
 }
 
+// Eviction from the key's H1 (victims are H1's own keys, whose H0 is H1) under H1's lock, taken
+// with a few attempts only: the caller already holds H0's lock.
+template <int P>
+__device__ __forceinline__ int try_evict_h1(const Table& t, u64* B1p, const Bucket& B1, uint32_t b1, u64 kv) {
+    if (!try_lock_bucket(t, b1)) return kEvNone;
+    const int ev = try_evict<P>(t, B1p, B1, b1, kv);
+    unlock_bucket(t, b1);
+    return ev;
+}
+
 // Stage C/D under H0's lock.  The caller holds the lock on b0.
 template <int P>
 __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
@@ -770,14 +793,32 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         int ev = try_evict<P>(t, B0p, B0, b0, kv);
         if (ev == kEvPlaced) return kStInserted;
         if (ev == kEvRetry) continue;
+        // No victim of H0 can move: the same with H1's own keys (keys whose H0 is H1), under H1's
+        // lock, and the key takes the freed slot in its H1.  Every invariant above still holds: a
+        // victim moves from its H0 to its H1, and the key lands in H1 while its H0 is full.  Tried
+        // before the stash for region-ordered batches (kFlagEvictH1), whose placement it keeps
+        // from overflowing stashes; otherwise only once the stash is full.
+        const bool h1_first = t.flags & kFlagEvictH1;
+        if (h1_first && b1 != b0) {
+            ev = try_evict_h1<P>(t, B1p, B1, b1, kv);
+            if (ev == kEvPlaced) return kStInserted;
+            if (ev == kEvRetry) continue;
+        }
         // Stage D: the canonical bucket's stash.  Its flag is raised before the entry is
         // written, so a reader that finds the entry also finds the flag set.
         if (!(atomicOr(t.stash_bits + (b0 >> 5), 1u << (b0 & 31)) & (1u << (b0 & 31)))) fence_acq_rel();
+        bool again = false;  // a last-resort eviction raced: rescan from the top
         for (int q = 0; q < kRetryLimit; ++q) {
             Bucket S;
             load_bucket(Sp, S);
             uint32_t se = empty_mask(S);
             if (!se) {
+                if (!h1_first && b1 != b0) {
+                    ev = try_evict_h1<P>(t, B1p, B1, b1, kv);
+                    if (ev == kEvPlaced) return kStInserted;
+                    again = ev == kEvRetry;
+                    if (again) break;
+                }
                 count(t, kCtrFailed);
                 return kStFail;
             }
@@ -787,6 +828,7 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
                 return kStStashed;
             }
         }
+        if (again) continue;
         break;
     }
     count(t, kCtrRetryOut);
@@ -806,24 +848,27 @@ __device__ __forceinline__ uint8_t update_slot(u64* p, int j, u64 cur, u64 kv) {
 }
 
 // Without holes and without tag upkeep (a bulk insert whose tag words are rebuilt after it):
-// update k in bucket b or claim b's lowest free slot from one 64 B read of the bucket.
+// update k in bucket b or claim b's lowest free slot from one 64 B read of the bucket.  Without
+// holes a slot never becomes free again, so after a lost CAS the next free slot of the same
+// snapshot is the next candidate: the bucket is read once however many claimers race for it (a
+// slot passed over was observed by its failed CAS, so a racing insert of k is always seen).
 // Returns kStUpdated / kStInserted, or 0 when b is full or a budget ran out.
 __device__ __forceinline__ uint8_t claim_or_update_untagged(const Table& t, uint32_t b, uint32_t k, u64 kv) {
     u64* p = t.slots + (size_t)b * kSlots;
-    for (int r = 0; r < kRetryLimit; ++r) {
-        Bucket B;
-        load_bucket(p, B);
-        const uint32_t m = match_mask(B, k);
-        if (m) {
-            const int j = __ffs(m) - 1;
-            return update_slot(p, j, slot_at(B, j), kv);
-        }
-        const uint32_t e = empty_mask(B);
-        if (!e) return 0;
+    Bucket B;
+    load_bucket(p, B);
+    const uint32_t m = match_mask(B, k);
+    if (m) {
+        const int j = __ffs(m) - 1;
+        return update_slot(p, j, slot_at(B, j), kv);
+    }
+    uint32_t e = empty_mask(B);
+    while (e) {
         const int j = __ffs(e) - 1;
+        e &= e - 1;
         const u64 obs = cas64(p + j, 0ull, kv);
         if (obs == 0ull) {
-            if (__popc(e) == 1) mark_full(t, b);
+            if (!e) mark_full(t, b);
             return kStInserted;
         }
         if (key_of(obs) == k) return update_slot(p, j, obs, kv);

@@ -208,7 +208,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, co
 // pass (sequential traffic), and at the end one scatter of the per-op outputs back to the
 // caller's order.
 // ---------------------------------------------------------------------------------------------
-constexpr int kMinRegionShift = 15;       // >= 32768 buckets = 2 MiB of slots per region
+// Regions of 2^15 .. 2^20 buckets (2 .. 64 MiB of slots), about 8 per table.  A region is the
+// span the blocks in flight share: small regions crowd ~7 concurrent claimers onto each bucket
+// (2 MiB regions ran a 2^26-slot insert at 7.6 ms against 4.9 ms with 64 MiB ones), while a 64 MiB
+// region still stays in L2.
+constexpr int kMinRegionShift = 15;
+constexpr int kMaxRegionShift = 20;
 constexpr int kMaxRegions = 1024;
 constexpr int kRegionTile = kBlock * 8;   // ops per block in the histogram and scatter passes
 
@@ -855,7 +860,9 @@ bool use_regions(const hive_table* h, uint64_t n, int knob) {
 // (synchronously) to the largest batch seen.
 int prepare_regions(hive_table* h, uint64_t n, int nsub, cudaStream_t s, Regions* r) {
     const uint64_t nb = num_buckets(h);
-    int sh = kMinRegionShift;
+    int lg = 0;
+    while ((2ull << lg) <= nb) ++lg;  // floor(log2(nb))
+    int sh = std::min(kMaxRegionShift, std::max(kMinRegionShift, lg - 3));
     while (((nb + (1ull << sh) - 1) >> sh) * (uint64_t)nsub > (uint64_t)kMaxRegions) ++sh;
     r->nsub = nsub;
     r->rshift = sh;
@@ -1229,9 +1236,14 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
     bool untag;
     if ((rc = insert_view(h, n, s, &tt, &untag))) return rc;
     if (use_regions(h, n, HIVE_TUNE_REGION_INSERT)) {
-        // region-ordered: sort, both passes over the sorted arrays, statuses back to caller order
+        // region-ordered: sort, both passes over the sorted arrays, statuses back to caller order.
+        // Knob 1: sub-batches with an H0-only first pass; knob 2: one pass claiming in H0 then H1,
+        // the locked path evicting from H1 before it uses the stash.
         Regions r;
-        const int nsub = insert_subbatches(h, n);
+        const bool single = h->tune[HIVE_TUNE_REGION_INSERT] == 2;
+        const int nsub = single ? 1 : insert_subbatches(h, n);
+        hive::Table tr = tt;
+        if (single) tr.flags |= hive::kFlagEvictH1;
         if ((rc = prepare_regions(h, n, nsub, s, &r)) || (rc = region_sort(h, keys, values, n, r, s))) return rc;
         for (int k = 0; k < nsub; ++k) {
             // sub-batch k holds ops i with i * nsub / n == k, i.e. [ceil(k n / nsub), ceil((k+1) n / nsub))
@@ -1240,9 +1252,9 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
             if (!m) continue;
             if (k && (rc = prepare_defer(h, m, s, &d))) return rc;
             uint8_t* rst = status ? r.rst + lo : nullptr;
-            launch_first_pass(h, tt, d, 0, m, s, r.rkeys + lo, r.rvals + lo, rst, true);
+            launch_first_pass(h, tr, d, 0, m, s, r.rkeys + lo, r.rvals + lo, rst, !single);
             if (d.q)
-                HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, m), kBlock, s, tt, r.rkeys + lo, r.rvals + lo, rst,
+                HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, m), kBlock, s, tr, r.rkeys + lo, r.rvals + lo, rst,
                               d);
         }
         if (untag) retag(h, s);
@@ -1666,7 +1678,7 @@ int hive_verify(hive_table* h, uint64_t* out, void* stream) {
 
 int hive_set_tuning(hive_table* h, int32_t key, int64_t value) {
     if (!valid_table(h) || key < 0 || key >= HIVE_NUM_TUNES) return HIVE_ERR_INVALID_ARG;
-    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0, 0}, hi[HIVE_NUM_TUNES] = {1, 1, 8, 8, 2, 2};
+    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0, 0}, hi[HIVE_NUM_TUNES] = {2, 1, 8, 8, 2, 2};
     if (value < lo[key] || value > hi[key]) return HIVE_ERR_INVALID_ARG;
     h->tune[key] = value;
     return HIVE_OK;

@@ -258,8 +258,10 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
  * Knobs of how a batch is run, never of what it computes: every setting gives the results of
  * the one-at-a-time replay.  They replace the reference's compile-time launch constants
  * (THREADS_PER_BLOCK / blocks-per-SM in src/hive_dispatch.cu) and are what an autotuner sets. */
-#define HIVE_TUNE_REGION_INSERT 0    /* 1: large inserts run in bucket-region order (a counting
-                                        sort first, statuses permuted back); 0 (default): in
+#define HIVE_TUNE_REGION_INSERT 0    /* large inserts in bucket-region order (a counting sort
+                                        first, statuses permuted back): 1 in sub-batches with an
+                                        H0-only first pass; 2 in one pass claiming H0 then H1,
+                                        evicting from H1 before the stash; 0 (default): in
                                         submission order                                        */
 #define HIVE_TUNE_REGION_FIND 1      /* the same for hive_find; default 0                       */
 #define HIVE_TUNE_SUBBATCHES 2       /* sub-batches of a region-ordered insert, 1..8; 0 (default)

@@ -112,23 +112,24 @@ def test_bulk_sweep(cuda, policy, cap_log, lf):
 
 
 @pytest.mark.parametrize("policy", POLICIES)
-@pytest.mark.parametrize("subbatches", [0, 1, 3, 8])
-def test_region_ordered_batches(cuda, policy, subbatches):
+@pytest.mark.parametrize("mode,subbatches", [(1, 0), (1, 1), (1, 3), (1, 8), (2, 0)])
+def test_region_ordered_batches(cuda, policy, mode, subbatches):
     """Region-ordered insert and find (counting sort by bucket region, statuses permuted back):
     same per-op results and the same final key set as the replay, at 2^18 buckets (the smallest
-    table that takes the region path) and LF 0.95."""
+    table that takes the region path) and LF 0.95.  Mode 1: sub-batches with an H0-only first
+    pass; mode 2: one pass claiming H0 then H1, evicting from H1 before the stash."""
     cap = 1 << 21
     n = int(0.95 * cap)
     keys, absent, st = oracle.gen_keys(11, n, 1 << 16)
     vals = oracle.values_for(keys)
     m = oracle.ReplayMap()
     with HiveHashTable(cap, policy) as t:
-        t.set_tuning(region_insert=1, region_find=1, subbatches=subbatches)
+        t.set_tuning(region_insert=mode, region_find=1, subbatches=subbatches)
         assert t.tuning()["subbatches"] == subbatches
         ins = _insert_and_check(t, m, keys, vals)
         failed = int((ins == ST_FAIL).sum())
         assert t.counters()["failed"] == failed
-        if subbatches in (0, 8):  # the automatic choice at this load is 8 sub-batches
+        if subbatches in (0, 8):  # the automatic choice (mode 1) at this load is 8 sub-batches
             assert failed == 0, failed
         # re-insert a slice with new values: updates in region order
         upd = keys[: n // 2][::-1].copy()
@@ -252,7 +253,7 @@ def test_tuning_bounds(cuda):
     with HiveHashTable(1 << 12) as t:
         assert t.tuning() == {"region_insert": 0, "region_find": 0, "subbatches": 0, "second_pass_blocks": 4,
                               "bulk_retag": 1, "tags": 1}
-        for bad in ({"region_insert": 2}, {"subbatches": 9}, {"second_pass_blocks": 0}, {"bulk_retag": 3},
+        for bad in ({"region_insert": 3}, {"subbatches": 9}, {"second_pass_blocks": 0}, {"bulk_retag": 3},
                     {"tags": 3}):
             with pytest.raises(HiveError):
                 t.set_tuning(**bad)
