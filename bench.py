@@ -192,6 +192,24 @@ def pcie_bandwidth(dev, nbytes=256 << 20, reps=4):
         b.record(s)
         torch.cuda.synchronize()
         out[name] = round(reps * nbytes / (a.elapsed_time(b) / 1e3) / 1e9, 1)
+    # both directions at once, as in the e2e step (uploads while results come back)
+    h2 = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d2 = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(up)
+    ev[2].record(down)
+    for _ in range(reps):
+        with torch.cuda.stream(up):
+            d.copy_(h, non_blocking=True)
+        with torch.cuda.stream(down):
+            h2.copy_(d2, non_blocking=True)
+    ev[1].record(up)
+    ev[3].record(down)
+    torch.cuda.synchronize()
+    out["h2d_duplex_gbs"] = round(reps * nbytes / (ev[0].elapsed_time(ev[1]) / 1e3) / 1e9, 1)
+    out["d2h_duplex_gbs"] = round(reps * nbytes / (ev[2].elapsed_time(ev[3]) / 1e3) / 1e9, 1)
     return out
 
 
@@ -322,10 +340,15 @@ def run_served(args, dev):
             r = serve(t, w.types, w.keys, w.vals, poisson_arrivals(n_req, 0), depth=4, max_batch=1 << 16)
             peak = r.summary()["mops"]
             runs = {"peak": {k: round(v, 4) if isinstance(v, float) else v for k, v in r.summary().items()}}
-            for frac in (0.1, 0.25, 0.5, 0.75, 0.9):
+            for frac in (0.1, 0.25, 0.5, 0.8, 0.9):
                 arr = poisson_arrivals(n_req, frac * peak * 1e6, seed=int(frac * 100))
                 s = serve(t, w.types, w.keys, w.vals, arr, depth=4, max_batch=1 << 16).summary()
                 runs[f"{frac:.2f}"] = {k: round(s[k], 4) for k in ("mops", "p50_ms", "p99_ms", "p999_ms")}
+            # the plain loop at the same offered load: one batch at a time (depth 1), so requests
+            # that arrive while a batch is on the GPU wait for it to finish
+            arr = poisson_arrivals(n_req, 0.8 * peak * 1e6, seed=80)
+            s = serve(t, w.types, w.keys, w.vals, arr, depth=1, max_batch=1 << 16).summary()
+            runs["0.80_plain_depth1"] = {k: round(s[k], 4) for k in ("mops", "p50_ms", "p99_ms", "p999_ms")}
             out["mixes"][mix] = runs
             t.check()
     return out
@@ -544,7 +567,9 @@ def main():
             ems = float(tt.item())
         assert int(fd_h.sum()) == n_present and int((st_h != 0).sum()) == n
         pcie = pcie_bandwidth(dev)
-        h2d_bound_ms = (n * 8 + n_look * 4) / (pcie["h2d_gbs"] * 1e9) * 1e3
+        # the step uploads while results come back, so the bound is the upload rate with both
+        # directions busy
+        h2d_bound_ms = (n * 8 + n_look * 4) / (pcie["h2d_duplex_gbs"] * 1e9) * 1e3
         e2e = {"value": round(2 * n * args.steps * world / (ems / 1e3) / 1e6, 2), "unit": UNIT,
                "pcie": pcie, "h2d_bound_ms": round(h2d_bound_ms, 3),
                "frac_of_h2d_bound": round(h2d_bound_ms / (ems / args.steps), 4),
