@@ -567,11 +567,14 @@ def main():
             ems = float(tt.item())
         assert int(fd_h.sum()) == n_present and int((st_h != 0).sum()) == n
         pcie = pcie_bandwidth(dev)
-        # the step uploads while results come back, so the bound is the upload rate with both
-        # directions busy
-        h2d_bound_ms = (n * 8 + n_look * 4) / (pcie["h2d_duplex_gbs"] * 1e9) * 1e3
+        # the uploads alone bound the step from below (one-way rate); with the results coming
+        # back at the same time, the upload rate falls towards the both-directions figure
+        up_bytes = n * 8 + n_look * 4
+        h2d_bound_ms = up_bytes / (pcie["h2d_gbs"] * 1e9) * 1e3
+        h2d_duplex_bound_ms = up_bytes / (pcie["h2d_duplex_gbs"] * 1e9) * 1e3
         e2e = {"value": round(2 * n * args.steps * world / (ems / 1e3) / 1e6, 2), "unit": UNIT,
                "pcie": pcie, "h2d_bound_ms": round(h2d_bound_ms, 3),
+               "h2d_duplex_bound_ms": round(h2d_duplex_bound_ms, 3),
                "frac_of_h2d_bound": round(h2d_bound_ms / (ems / args.steps), 4),
                "h2d_bytes_per_step": int(n * 8 + n_look * 4), "d2h_bytes_per_step": int(n + n_look * 5),
                "ms_per_step": round(ems / args.steps, 4), "api": "HiveHashTable.insert_host + find_host",

@@ -11,9 +11,10 @@
 //                                keeps this as bit 31 of a per-bucket freeMask word,
 //                                include/hive_hash_insert.cuh:512-514); 1 bit per bucket keeps
 //                                it L2-resident (1 MiB at 2^23 buckets)
-//   locks      u32[nb_cap]       eviction locks, one word per bucket as in the reference
-//                                (include/hive_hash_table_struct.cuh:101-117): a word per bucket
-//                                keeps evictors of unrelated buckets off each other's words
+//   locks      u8[nb_cap]        eviction locks, one byte per bucket (the reference keeps a word
+//                                per bucket, include/hive_hash_table_struct.cuh:101-117): 8 MiB
+//                                at 2^23 buckets, so the locked path's lock updates stay in L2;
+//                                a byte is set with a CAS on its 32-bit word
 //   full_bits  u32[nb_cap / 32]  bit b set = bucket b was seen full (set by the claim that took
 //                                its last free slot, cleared by deletes).  A hint only: the
 //                                evictor reads it for all 8 victims' alternate buckets at once
@@ -68,6 +69,7 @@ enum {
     kCtrLockTimeout = 4,  // lock waits that expired
     kCtrRetryOut = 5,     // CAS retry budgets that ran out
     kCtrDupFixed = 6,     // duplicate copies removed after racing same-key inserts
+    kCtrLockWaits = 7,    // lock attempts that found the bucket locked (contention)
     kCtrError = 15,       // sticky error bits (kErr*)
 };
 enum : unsigned long long { kErrLockTimeout = 1ull, kErrRetryOut = 2ull };
@@ -90,7 +92,7 @@ struct Table {
     u64* slots;
     u64* stash;
     uint32_t* stash_bits;
-    uint32_t* locks;
+    uint32_t* locks;  // lock bytes, 4 per word
     uint32_t* full_bits;
     u64* counters;
     u64* tags;
@@ -308,7 +310,22 @@ __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gp
 constexpr int kRetryLimit = 64;       // CAS retries of one op on one bucket
 constexpr int kLockSpinLimit = 1 << 16;  // lock attempts before the wait is declared expired
 
-// Bounded test-and-set on the bucket's lock word.  Returns false when the wait expired.
+// Set bucket b's lock byte if it is clear: a CAS on the word holding it, retried while only the
+// other bytes (other buckets' locks) change.  Returns true when taken, false when the byte is set.
+__device__ __forceinline__ bool lock_byte_try(const Table& t, uint32_t b) {
+    uint32_t* w = t.locks + (b >> 2);
+    const uint32_t bit = 1u << (8 * (b & 3));
+    uint32_t old = ld_relaxed_u32(w);
+    for (int r = 0; r < kRetryLimit; ++r) {
+        if (old & bit) return false;
+        const uint32_t obs = atomicCAS(w, old, old | bit);
+        if (obs == old) return true;
+        old = obs;
+    }
+    return false;
+}
+
+// Bounded test-and-set on the bucket's lock byte.  Returns false when the wait expired.
 //
 // The lock only excludes other evictors of the same bucket; every table access made while it is
 // held is itself a gpu-scope CAS or a strong (ld.relaxed.gpu) load, each completed (its result
@@ -319,7 +336,8 @@ constexpr int kLockSpinLimit = 1 << 16;  // lock attempts before the wait is dec
 __device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
     unsigned ns = 32;
     for (int i = 0; i < kLockSpinLimit; ++i) {
-        if (atomicCAS(t.locks + b, 0u, 1u) == 0u) return true;
+        if (lock_byte_try(t, b)) return true;
+        count(t, kCtrLockWaits);
         __nanosleep(ns);
         if (ns < 1024) ns <<= 1;
     }
@@ -327,13 +345,15 @@ __device__ __forceinline__ bool lock_bucket(const Table& t, uint32_t b) {
     raise_error(t, kErrLockTimeout);
     return false;
 }
-__device__ __forceinline__ void unlock_bucket(const Table& t, uint32_t b) { atomicExch(t.locks + b, 0u); }
+__device__ __forceinline__ void unlock_bucket(const Table& t, uint32_t b) {
+    atomicAnd(t.locks + (b >> 2), ~(1u << (8 * (b & 3))));
+}
 
 // A few attempts at the lock of a second bucket while the first one is held: never waits long,
 // so two evictors that each hold one of the pair and want the other cannot block each other.
 __device__ __forceinline__ bool try_lock_bucket(const Table& t, uint32_t b) {
     for (int i = 0; i < 4; ++i) {
-        if (atomicCAS(t.locks + b, 0u, 1u) == 0u) return true;
+        if (lock_byte_try(t, b)) return true;
         __nanosleep(64);
     }
     return false;

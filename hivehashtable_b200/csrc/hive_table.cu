@@ -114,7 +114,7 @@ Carve carve(uint64_t nb_cap) {
     c.stash = align256(c.slots + (size_t)nb_cap * 64);
     c.sbits = align256(c.stash + (size_t)nb_cap * 64);
     c.lbits = align256(c.sbits + words * 4);
-    c.fbits = align256(c.lbits + (size_t)nb_cap * 4);
+    c.fbits = align256(c.lbits + ((size_t)nb_cap + 3) / 4 * 4);  // lock bytes
     c.ctr = align256(c.fbits + words * 4);
     c.tags = align256(c.ctr + kCounterBytes);
     c.scratch = align256(c.tags + (size_t)nb_cap * 8);
@@ -143,19 +143,25 @@ void bind_arrays(hive_table* h, void* block, uint64_t nb_cap) {
 // ---------------------------------------------------------------------------------------------
 
 // The queue of ops deferred by a first pass to the second (insert stages C/D): op indices and
-// their count.  q == nullptr disables deferral.
+// their count.  q == nullptr disables deferral.  permute: visit the queue in a permuted order.
 struct Defer {
     uint32_t* q;
     u64* n;
+    uint32_t permute = 0;
 };
 
-// The second pass visits queue position defer_slot(j, cnt) at step j: a bijection of [0, cnt)
-// (multiplication by a prime larger than any queue), so the deferred ops -- appended in the
-// first pass's order, which for a region-ordered batch is bucket order -- are finished in an
-// order unrelated to their buckets.  Finished in bucket order, the last buckets' overflow would
+// The second pass visits queue position defer_slot(j, cnt) at step j.  In submission order the
+// queue is already in random bucket order and is visited in order: consecutive queue entries hold
+// increasing op indices, so the keys, values and statuses they name are read and written nearly
+// sequentially (a permuted visit made them random accesses, the pass's largest cost).  A
+// region-ordered batch's queue is in bucket order; it is visited through a bijection of [0, cnt)
+// (multiplication by a prime larger than any queue) so that its deferred ops are finished in an
+// order unrelated to their buckets: finished in bucket order, the last buckets' overflow would
 // meet alternate buckets already filled by all earlier overflow and exhaust their stashes.
 // (j < cnt < 2^32, so j * (p mod cnt) < 2^64; gcd(p mod cnt, cnt) = gcd(p, cnt) = 1.)
-__device__ __forceinline__ u64 defer_slot(u64 j, u64 cnt) { return (j * (4294967311ull % cnt)) % cnt; }
+__device__ __forceinline__ u64 defer_slot(u64 j, u64 cnt, uint32_t permute) {
+    return permute ? (j * (4294967311ull % cnt)) % cnt : j;
+}
 
 // Appends index i for every lane whose st is kStDefer, one atomic per warp.  Every lane of the
 // warp must call it.
@@ -192,7 +198,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, co
                                                             uint8_t* __restrict__ status, Defer d) {
     const u64 cnt = *d.n;
     for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
-        const uint32_t i = d.q[defer_slot(j, cnt)];
+        const uint32_t i = d.q[defer_slot(j, cnt, d.permute)];
         const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals[i]);
         if (status) status[i] = st;
     }
@@ -390,7 +396,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_deferred(hive::Table t, con
                                                            Defer d) {
     const u64 cnt = *d.n;
     for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
-        const uint32_t i = d.q[defer_slot(j, cnt)];
+        const uint32_t i = d.q[defer_slot(j, cnt, d.permute)];
         const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals ? vals[i] : 0u);
         if (status) status[i] = st;
         if (outv) outv[i] = 0u;
@@ -430,7 +436,7 @@ __global__ void k_apply_batches(hive::Table t, const uint8_t* __restrict__ types
         const u64 cnt = *d.n;
         if (tid == 0) qn[(b + 1) & 1] = 0;
         for (u64 j = tid; j < cnt; j += stride) {
-            const uint32_t i = q[defer_slot(j, cnt)];
+            const uint32_t i = q[defer_slot(j, cnt, 0)];
             const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals ? vals[i] : 0u);
             if (status) status[i] = st;
             if (outv) outv[i] = 0u;
@@ -466,7 +472,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_apply_ref_deferred(hive::Table t,
                                                                unsigned long long* __restrict__ results, Defer d) {
     const u64 cnt = *d.n;
     for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
-        const uint32_t i = d.q[defer_slot(j, cnt)];
+        const uint32_t i = d.q[defer_slot(j, cnt, d.permute)];
         const uint32_t k = (uint32_t)ops[i].y;
         const uint8_t st = hive::insert_deferred_one<P>(t, k, k + 1u);
         if (results) results[i] = ref_result(st);
@@ -773,7 +779,7 @@ int reset(hive_table* h, cudaStream_t s) {
     int rc = launch_check();
     if (rc) return rc;
     HIVE_CUDA(cudaMemsetAsync(h->t.stash_bits, 0, (size_t)words * 4, s));
-    HIVE_CUDA(cudaMemsetAsync(h->t.locks, 0, (size_t)nb * 4, s));
+    HIVE_CUDA(cudaMemsetAsync(h->t.locks, 0, (size_t)(nb + 3) / 4 * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.full_bits, 0, (size_t)words * 4, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.counters, 0, kCounterBytes, s));
     HIVE_CUDA(cudaMemsetAsync(h->t.tags, 0, (size_t)nb * 8, s));
@@ -1251,6 +1257,7 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
             const uint64_t m = hi - lo;
             if (!m) continue;
             if (k && (rc = prepare_defer(h, m, s, &d))) return rc;
+            d.permute = 1;  // the queue is in bucket order
             uint8_t* rst = status ? r.rst + lo : nullptr;
             launch_first_pass(h, tr, d, 0, m, s, r.rkeys + lo, r.rvals + lo, rst, !single);
             if (d.q)

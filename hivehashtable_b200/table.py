@@ -37,7 +37,7 @@ HINT_LOOKUPS_ONLY = 2
 HINT_UNIQUE_KEYS = 4
 NUM_COUNTERS = 16
 COUNTER_NAMES = {0: "slow_path", 1: "evictions", 2: "stash_push", 3: "failed", 4: "lock_timeout",
-                 5: "retry_out", 6: "dup_fixed", 15: "error_bits"}
+                 5: "retry_out", 6: "dup_fixed", 7: "lock_waits", 15: "error_bits"}
 # Launch-tuning knobs (HIVE_TUNE_*): how a batch runs, never what it computes
 TUNES = {"region_insert": 0, "region_find": 1, "subbatches": 2, "second_pass_blocks": 3, "bulk_retag": 4,
          "tags": 5}

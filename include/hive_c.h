@@ -77,6 +77,7 @@ extern "C" {
 #define HIVE_CTR_LOCK_TIMEOUT 4 /* bucket-lock waits that expired                              */
 #define HIVE_CTR_RETRY_OUT 5    /* CAS retry budgets that ran out                              */
 #define HIVE_CTR_DUP_FIXED 6    /* duplicate copies removed after racing same-key inserts      */
+#define HIVE_CTR_LOCK_WAITS 7   /* bucket-lock attempts that found the lock taken (contention) */
 #define HIVE_CTR_ERROR 15       /* sticky error bits                                           */
 #define HIVE_NUM_COUNTERS 16
 
