@@ -1683,6 +1683,15 @@ int hive_verify(hive_table* h, uint64_t* out, void* stream) {
     return HIVE_OK;
 }
 
+int hive_debug_hold_lock(hive_table* h, uint64_t bucket, int held, void* stream) {
+    if (!valid_table(h) || bucket >= num_buckets(h) || (held != 0 && held != 1)) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    if (!g.ok) return HIVE_ERR_CUDA;
+    // the lock byte of `bucket` (byte b & 3 of word b >> 2; little-endian)
+    HIVE_CUDA(cudaMemsetAsync((char*)h->t.locks + bucket, held, 1, (cudaStream_t)stream));
+    return HIVE_OK;
+}
+
 int hive_set_tuning(hive_table* h, int32_t key, int64_t value) {
     if (!valid_table(h) || key < 0 || key >= HIVE_NUM_TUNES) return HIVE_ERR_INVALID_ARG;
     static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0, 0}, hi[HIVE_NUM_TUNES] = {2, 1, 8, 8, 2, 2};

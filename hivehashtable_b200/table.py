@@ -96,6 +96,7 @@ ABI = [
     ("hive_counters", _I32, [_P, _P, _P]),
     ("hive_check", _I32, [_P, _P]),
     ("hive_verify", _I32, [_P, _P, _P]),
+    ("hive_debug_hold_lock", _I32, [_P, _U64, _I32, _P]),
     ("hive_set_tuning", _I32, [_P, _I32, ctypes.c_int64]),
     ("hive_get_tuning", _I32, [_P, _I32, ctypes.POINTER(ctypes.c_int64)]),
     ("hive_strerror", ctypes.c_char_p, [_I32]),
@@ -380,6 +381,11 @@ class HiveHashTable:
         _check(self._lib.hive_verify(self._h, ctypes.cast(buf, ctypes.c_void_p), self._stream(stream)),
                "hive_verify")
         return {name: int(buf[i]) for i, name in enumerate(("tag_mismatch", "misplaced", "duplicate", "stale_tag"))}
+
+    def debug_hold_lock(self, bucket: int, held: bool = True, stream=None) -> None:
+        """Test hook: hold (or release) a bucket's eviction lock (hive_debug_hold_lock)."""
+        _check(self._lib.hive_debug_hold_lock(self._h, int(bucket), int(bool(held)), self._stream(stream)),
+               "hive_debug_hold_lock")
 
     def set_tuning(self, **knobs) -> None:
         """set_tuning(region_insert=1, subbatches=4, ...): see TUNES."""

@@ -285,6 +285,13 @@ int hive_set_tuning(hive_table* t, int32_t key, int64_t value);
 /* Read knob `key` into *value. */
 int hive_get_tuning(const hive_table* t, int32_t key, int64_t* value);
 
+/* Test hook for the bounded lock wait: held = 1 sets bucket `bucket`'s eviction lock as an
+ * evictor holding it would, held = 0 clears it (stream-ordered).  An insert that needs a held lock
+ * waits about 65 ms (2^16 attempts with a backoff), then returns HIVE_ST_ERROR for that op and
+ * sets the sticky HIVE_ERR_LOCK_TIMEOUT that hive_check reports.  No counterpart in the reference,
+ * whose lock spins are unbounded (include/hive_hash_table_struct.cuh:101-117). */
+int hive_debug_hold_lock(hive_table* t, uint64_t bucket, int held, void* stream);
+
 /* Message for a status code; never NULL. */
 const char* hive_strerror(int status);
 
