@@ -78,6 +78,8 @@ constexpr uint32_t kFlagHoles = 1u;     // deletes or a resize ran since the las
 constexpr uint32_t kFlagEvictH1 = 4u;   // set on the launch's copy only: the locked path tries
                                         // H1's own keys as victims before the stash (region-
                                         // ordered batches), not only once the stash is full
+constexpr uint32_t kFlagPrimaryFirst = 8u;  // set on the launch's copy only: its first pass
+                                            // claimed in H0 only (region order, sub-batches)
 constexpr uint32_t kFlagUntagged = 2u;  // set on the launch's copy only: the launch neither reads
                                         // nor keeps the tag words (a bulk insert that rebuilds them
                                         // after it, or a table too large for them to stay in L2)
@@ -1124,16 +1126,19 @@ __device__ __forceinline__ uint8_t insert_one(const Table& t, uint32_t k, uint32
     return insert_locked_path<P>(t, k, kv, b0, b1);
 }
 
-// A deferred op in the second pass.  Without holes its H0 was full in the first pass and stays
-// full, so it claims (or updates) in H1 without a lock and takes the locked path only if H1 is
-// full too; with holes the whole protocol runs again (a slot may have freed up since).
+// A deferred op in the second pass.  Without holes the buckets the first pass found full stay
+// full; with holes the whole protocol runs again (a slot may have freed up since).
 template <int P>
 __device__ __forceinline__ uint8_t insert_deferred_one(const Table& t, uint32_t k, uint32_t v) {
     if (t.flags & kFlagHoles) return insert_one<P>(t, k, v);
     const u64 kv = pack(k, v);
     const uint32_t b0 = bucket_addr(t, Policy<P>::h0(k));
     const uint32_t b1 = bucket_addr(t, Policy<P>::h1(k));
-    if (b1 != b0) {
+    // A first pass that also claimed in H1 deferred the op because both buckets were full, and
+    // without holes they stay full: the locked path follows directly (it rescans both buckets
+    // under the lock, which also finds a racing insert of k).  After an H0-only first pass the
+    // op claims in H1 first.
+    if (b1 != b0 && (t.flags & kFlagPrimaryFirst)) {
         const uint8_t st = tagged(t) ? claim_or_update<true>(t, b1, k, kv) : claim_or_update<false>(t, b1, k, kv);
         if (st) return st;
     }

@@ -1249,7 +1249,7 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
         const bool single = h->tune[HIVE_TUNE_REGION_INSERT] == 2;
         const int nsub = single ? 1 : insert_subbatches(h, n);
         hive::Table tr = tt;
-        if (single) tr.flags |= hive::kFlagEvictH1;
+        tr.flags |= single ? hive::kFlagEvictH1 : hive::kFlagPrimaryFirst;
         if ((rc = prepare_regions(h, n, nsub, s, &r)) || (rc = region_sort(h, keys, values, n, r, s))) return rc;
         for (int k = 0; k < nsub; ++k) {
             // sub-batch k holds ops i with i * nsub / n == k, i.e. [ceil(k n / nsub), ceil((k+1) n / nsub))
