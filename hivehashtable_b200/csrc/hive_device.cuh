@@ -638,14 +638,15 @@ __device__ __forceinline__ bool resolve_duplicate(const Table& t, uint32_t b, ui
 //   A  try-replace in the candidate buckets and the canonical stash,
 //   B  claim a free slot with a 64-bit CAS: in the canonical bucket H0, and when H0 is full in
 //      the key's other bucket H1 (the reference claims in H0 only and goes straight to C),
-//   C  bounded depth-1 cuckoo eviction from H0 under H0's lock,
+//   C  bounded depth-1 cuckoo eviction from H0 under H0's lock (and of H1's own keys under H1's
+//      lock: before the stash for region-ordered batches, else once the stash is full),
 //   D  the canonical bucket's overflow stash.
 //
 // Invariants that keep every key in exactly one place and visible at all times:
 //   * a new key is placed in H0, in H1 only when H0 is full, else in H0's stash;
 //   * a victim is moved only from its own H0 to its H1, and is written to H1 before its H0 slot
 //     is overwritten, so a reader scanning H0 then H1 always sees it;
-//   * an evictor holds H0's lock, so one victim has one mover;
+//   * an evictor holds the lock of the victim's own bucket (its H0), so one victim has one mover;
 //   * every slot change is a CAS from an observed value, so a concurrent update or delete of
 //     the victim is detected and either propagated to the copy or undone.
 // Without kFlagHoles (no delete or resize since the last clear) slots only ever go from free to
