@@ -16,9 +16,17 @@
 //   pipeline   up to `depth` batches are in flight: while the GPU works on one, the next batch is
 //              formed, copied and queued.  depth = 1 is the plain loop: one synchronous batch at
 //              a time
-//   growth     before a batch that could push the load factor past max_load, the loop drains,
-//              checks free device memory for the doubled table (cudaMemGetInfo) and grows it
-//              with hive_resize; when memory does not allow it, the batch's new keys are refused
+//   growth     the load is tracked without touching the device: keys known placed (from the
+//              statuses of finished batches) plus every distinct write in flight counted as new.
+//              Loads count against the slots of the unsplit level (8 n_lo; see level_slots).
+//              Incremental (grow_start > 0): once the load could pass grow_start, the loop sets a
+//              target of the next full level and, before each batch, splits the next run of buckets
+//              toward it on the compute stream (hive_resize within the reservation queues the
+//              split kernel and returns), so batches keep flowing; the run length makes the
+//              doubling end within the batches that fit between grow_start and max_load.  At once
+//              (fallback): before a batch that could push the load past max_load, the loop drains,
+//              recounts, checks free device memory for the next level (cudaMemGetInfo) and
+//              grows to it.  When memory does not allow growth, the batch's new keys are refused
 //              (status 0) and existing keys still update
 //
 // Completion time of a request = when its batch's results are on the host and answered.
@@ -26,6 +34,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -101,8 +110,33 @@ struct Slot {
     std::vector<int32_t> find_of;     // group -> position in the lookup list or -1
     std::vector<int32_t> upsert_of;   // group -> position in the upsert list or -1
     uint32_t nf = 0, nu = 0;
+    uint64_t new_writes = 0;          // distinct written keys of the batch (possible new keys)
     bool busy = false;
 };
+
+// Device bytes per bucket of a table allocation (8 slots, 8 stash entries, fingerprint word,
+// lock byte, stash and full bits), rounded up.
+constexpr double kBytesPerBucket = 140.0;
+
+// Smallest split step of incremental growth (buckets): below this a step costs more in launch
+// overhead than it moves.
+constexpr uint64_t kMinGrowStep = 1u << 10;
+
+// Mid-level, a bucket not yet split takes keys of 1/n_lo of the hash space, twice a split
+// bucket's share, so the load that bounds placement is keys / (8 n_lo): the capacity that growth
+// decisions count is that of the level, and growth targets the next full level (2 n_lo buckets).
+uint64_t level_buckets(const hive_info& info) { return (uint64_t)info.base_buckets << info.level; }
+double level_slots(const hive_info& info) { return 8.0 * (double)level_buckets(info); }
+
+// Whether the table may grow to `target` buckets: within the reservation always; beyond it when
+// free device memory holds the new allocation (the old one stays until the copy is done).
+bool growth_admitted(const hive_info& info, uint64_t target) {
+    if (target <= info.max_buckets) return true;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+    const double nb_cap = (double)std::max<uint64_t>(target, 2 * info.max_buckets);
+    return (double)fr > nb_cap * kBytesPerBucket * 1.05;
+}
 
 int alloc_slot(Slot& s, uint32_t cap) {
     if (cudaStreamCreateWithFlags(&s.copy, cudaStreamNonBlocking) != cudaSuccess) return HIVE_ERR_CUDA;
@@ -146,6 +180,8 @@ int hive_serve_run(
     if (!t || !cfg || !types || !keys || !vals || !arrival_s || !out_vals || !out_status || !done_s)
         return HIVE_ERR_INVALID_ARG;
     if (cfg->depth < 1 || cfg->depth > 64 || cfg->max_batch < 1) return HIVE_ERR_INVALID_ARG;
+    if (!(cfg->grow_start >= 0.0) || (cfg->grow_start > 0.0 && !(cfg->grow_start < cfg->max_load)))
+        return HIVE_ERR_INVALID_ARG;
     hive_serve_stats st{};
     const uint32_t cap = cfg->max_batch;
     std::vector<Slot> slots(cfg->depth);
@@ -155,7 +191,10 @@ int hive_serve_run(
     for (auto& s : slots)
         if ((rc = alloc_slot(s, cap))) break;
     hive_info info{};
-    uint64_t live = cfg->live_keys;
+    uint64_t live_done = cfg->live_keys;  // keys in the table after the finished batches
+    uint64_t pending_new = 0;             // possible new keys of the batches in flight
+    uint64_t grow_target = 0, grow_step = 0;  // incremental growth: target buckets, buckets per step
+    uint64_t grow_refused_at = 0;             // bucket count at which growth found no memory
 
     GroupMap gid(cap);
     std::vector<uint32_t> g_key;    // group -> key
@@ -191,6 +230,10 @@ int hive_serve_run(
                 out_vals[r] = 0;
             }
         }
+        uint64_t placed_new = 0;
+        for (uint32_t u = 0; u < s.nu; ++u) placed_new += s.h_ust[u] == HIVE_ST_INSERTED || s.h_ust[u] == HIVE_ST_STASHED;
+        live_done += placed_new;
+        pending_new -= s.new_writes;
         const double td = now_s();
         std::fill(done_s + s.first, done_s + s.first + s.count, td);
         finished += s.count;
@@ -276,28 +319,65 @@ int hive_serve_run(
                 s.upsert_of[g] = (int32_t)s.nu++;
             }
         }
-        // growth: keep the load factor under max_load counting every write as a possible new key
+        // growth: keep the load factor under max_load counting every write in flight as a new key
         if (cfg->max_load > 0.0 && new_writes) {
             hive_get_info(t, &info);
-            const double cap_slots = (double)info.capacity_slots;
-            if ((double)(live + new_writes) > cfg->max_load * cap_slots) {
+            const uint64_t est = live_done + pending_new + new_writes;
+            if (cfg->grow_start > 0.0) {
+                if (!grow_target && info.num_buckets != grow_refused_at &&
+                    (double)est > cfg->grow_start * level_slots(info)) {
+                    const uint64_t target = 2 * level_buckets(info);
+                    if (growth_admitted(info, target)) {
+                        // batches that fit between grow_start and max_load of the level; the
+                        // doubling is spread over half of them
+                        const double room = (cfg->max_load - cfg->grow_start) * level_slots(info);
+                        const double batches = std::max(1.0, std::floor(room / (double)cap / 2.0));
+                        grow_target = target;
+                        grow_step = std::max<uint64_t>(kMinGrowStep,
+                                                       (uint64_t)std::ceil((target - info.num_buckets) / batches));
+                    } else {
+                        grow_refused_at = info.num_buckets;
+                    }
+                }
+                if (grow_target) {
+                    const uint64_t to = std::min(grow_target, info.num_buckets + grow_step);
+                    if ((rc = hive_resize(t, to * 8, compute))) {
+                        if (rc == HIVE_ERR_CUDA) break;
+                        rc = HIVE_OK;  // no memory for it after all: leave it to the check below
+                        grow_refused_at = info.num_buckets;
+                        grow_target = 0;
+                    } else {
+                        ++st.grow_steps;
+                        if (to == grow_target) {
+                            grow_target = 0;
+                            ++st.resizes;
+                        }
+                    }
+                    hive_get_info(t, &info);
+                }
+            }
+            const double cap_slots = level_slots(info);
+            if ((double)est > cfg->max_load * cap_slots) {
                 if ((rc = drain())) break;
                 uint64_t sz = 0;
                 if ((rc = hive_size(t, &sz, compute))) break;
-                live = sz;
-                if ((double)(live + new_writes) > cfg->max_load * cap_slots) {
-                    size_t fr = 0, tot = 0;
-                    cudaMemGetInfo(&fr, &tot);
-                    const double need = cap_slots / 8.0 * 140.0 * 1.1;  // slots+stash+metadata of the doubled part
-                    if ((double)fr > need && hive_resize(t, info.capacity_slots * 2, compute) == HIVE_OK) {
+                live_done = sz;
+                if ((double)(live_done + new_writes) > cfg->max_load * cap_slots) {
+                    ++st.drains;
+                    const uint64_t target = 2 * level_buckets(info);
+                    if (info.num_buckets != grow_refused_at && growth_admitted(info, target) &&
+                        hive_resize(t, target * 8, compute) == HIVE_OK) {
                         ++st.resizes;
+                        grow_target = 0;
                     } else {
+                        grow_refused_at = info.num_buckets;
                         st.refused += new_writes;  // the batch still runs; inserts that find no room fail
                     }
                 }
             }
         }
-        live += new_writes;
+        pending_new += new_writes;
+        s.new_writes = new_writes;
         // launch
         if (s.nf && cudaMemcpyAsync(s.d_fkeys, s.h_fkeys, (size_t)s.nf * 4, cudaMemcpyHostToDevice, s.copy)) rc = HIVE_ERR_CUDA;
         if (s.nu && (cudaMemcpyAsync(s.d_ukeys, s.h_ukeys, (size_t)s.nu * 4, cudaMemcpyHostToDevice, s.copy) ||

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -28,6 +29,7 @@ thread_local int g_last_cuda_error = 0;
 
 constexpr int kBlock = 256;
 constexpr double kMaxShrinkLoad = 0.9;
+constexpr uint64_t kLoadChunk = 1ull << 22;  // entries per insert of hive_load
 
 inline int cuda_fail(cudaError_t e) {
     g_last_cuda_error = (int)e;
@@ -584,6 +586,25 @@ __global__ void k_dump(hive::Table t, uint64_t nb, u64* __restrict__ kv, uint64_
                 }
         }
     }
+}
+
+// Splits packed entries ((value << 32) | key) into the key and value arrays an insert takes.
+__global__ void __launch_bounds__(kBlock) k_unpack(const u64* __restrict__ kv, uint64_t n, uint32_t* __restrict__ keys,
+                                                   uint32_t* __restrict__ vals) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const u64 e = kv[i];
+        keys[i] = (uint32_t)e;
+        vals[i] = (uint32_t)(e >> 32);
+    }
+}
+
+// *cnt += the ops of status[0, n) that were not placed (HIVE_ST_FAIL or HIVE_ST_ERROR).
+__global__ void __launch_bounds__(kBlock) k_count_unplaced(const uint8_t* __restrict__ status, uint64_t n, u64* cnt) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool bad = i < n && (status[i] == HIVE_ST_FAIL || status[i] == HIVE_ST_ERROR);
+    const unsigned m = __ballot_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(cnt, (u64)__popc(m));
 }
 
 // Structural check of buckets [0, nb) and their stashes; out[HIVE_VERIFY_*] counts violations:
@@ -1601,6 +1622,54 @@ int hive_dump(hive_table* h, uint64_t* kv, uint64_t cap, uint64_t* n_out, void* 
     HIVE_CUDA(cudaStreamSynchronize(s));
     *n_out = v;
     return HIVE_OK;
+}
+
+int hive_load(hive_table* h, const uint64_t* kv, uint64_t n, uint64_t* n_unplaced, void* stream) {
+    if (!valid_table(h) || (n && !kv)) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n_unplaced) *n_unplaced = 0;
+    // empty the table at its current geometry (hive_clear would also return it to level 0)
+    int rc = reset(h, s);
+    if (rc) return rc;
+    // Mid-level, a bucket not yet split takes keys of 1/n_lo of the hash space, twice a split
+    // bucket's share, so the load that bounds placement is n / (8 n_lo).  Grow (the table is
+    // empty, so the split kernels move nothing) to the first full level that keeps it at
+    // kMaxShrinkLoad.
+    uint64_t lvl = h->t.n_lo;
+    while ((double)n > kMaxShrinkLoad * (double)(lvl * hive::kSlots)) lvl *= 2;
+    if (lvl > h->t.n_lo && (rc = hive_resize(h, lvl * hive::kSlots, stream))) return rc;
+    h->t.flags = 0;  // an empty table has no holes, whatever resized it
+    h->tags_valid = true;
+    if (!n) return HIVE_OK;
+    // chunks through one temporary staging area: keys, values, statuses, the unplaced count
+    const uint64_t chunk = std::min<uint64_t>(n, kLoadChunk);
+    const size_t w = align256((size_t)chunk * 4);
+    char* tmp = nullptr;
+    cudaError_t e = cudaMalloc(&tmp, 2 * w + align256((size_t)chunk) + 256);
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? HIVE_ERR_OOM : cuda_fail(e);
+    uint32_t* keys = (uint32_t*)tmp;
+    uint32_t* vals = (uint32_t*)(tmp + w);
+    uint8_t* st = (uint8_t*)(tmp + 2 * w);
+    u64* cnt = (u64*)(tmp + 2 * w + align256((size_t)chunk));
+    u64 unplaced = 0;
+    if ((e = cudaMemsetAsync(cnt, 0, 8, s)) != cudaSuccess) rc = cuda_fail(e);
+    for (uint64_t off = 0; !rc && off < n; off += chunk) {
+        const uint64_t m = std::min(chunk, n - off);
+        k_unpack<<<grid_for(m), kBlock, 0, s>>>((const u64*)kv + off, m, keys, vals);
+        if ((rc = launch_check()) || (rc = hive_insert(h, keys, vals, m, st, stream))) break;
+        k_count_unplaced<<<grid_for(m), kBlock, 0, s>>>(st, m, cnt);
+        rc = launch_check();
+    }
+    if (!rc && (e = cudaMemcpyAsync(&unplaced, cnt, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) rc = cuda_fail(e);
+    if (!rc && (e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e);
+    // the staging area is only freed once the stream has finished with it
+    if (rc) cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    if (rc) return rc;
+    if (n_unplaced) *n_unplaced = unplaced;
+    if ((rc = hive_check(h, stream))) return rc;
+    return unplaced ? HIVE_ERR_CAPACITY : HIVE_OK;
 }
 
 int hive_resize(hive_table* h, uint64_t target_slots, void* stream) {

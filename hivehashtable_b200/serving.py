@@ -24,13 +24,13 @@ MIXES = {"A": 0, "B": 1, "C": 2, "D": 3}  # 50/50 lookup/update, 95/5, 100 % loo
 
 class ServeConfig(ctypes.Structure):
     _fields_ = [("depth", ctypes.c_uint32), ("max_batch", ctypes.c_uint32), ("max_load", ctypes.c_double),
-                ("live_keys", ctypes.c_uint64)]
+                ("live_keys", ctypes.c_uint64), ("grow_start", ctypes.c_double)]
 
 
 class ServeStats(ctypes.Structure):
     _fields_ = [("batches", ctypes.c_uint64), ("device_lookups", ctypes.c_uint64),
                 ("device_upserts", ctypes.c_uint64), ("resizes", ctypes.c_uint64), ("refused", ctypes.c_uint64),
-                ("wall_s", ctypes.c_double)]
+                ("wall_s", ctypes.c_double), ("grow_steps", ctypes.c_uint64), ("drains", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -101,7 +101,9 @@ class ServeResult:
 
 
 def serve(table: HiveHashTable, types, keys, vals, arrival, depth: int = 4, max_batch: int = 1 << 14,
-          max_load: float = 0.9, live_keys: Optional[int] = None) -> ServeResult:
+          max_load: float = 0.9, live_keys: Optional[int] = None, grow_start: Optional[float] = None) -> ServeResult:
+    """Run the request stream through the native loop.  Growth is incremental from `grow_start`
+    (default 0.8 * max_load; 0 = off, grow at once after a drain when max_load would be passed)."""
     types = np.ascontiguousarray(types, dtype=np.uint8)
     keys = np.ascontiguousarray(keys, dtype=np.uint32)
     vals = np.ascontiguousarray(vals, dtype=np.uint32)
@@ -110,7 +112,9 @@ def serve(table: HiveHashTable, types, keys, vals, arrival, depth: int = 4, max_
     out_v = np.zeros(n, dtype=np.uint32)
     out_s = np.zeros(n, dtype=np.uint8)
     done = np.zeros(n, dtype=np.float64)
-    cfg = ServeConfig(depth, max_batch, max_load, table.size() if live_keys is None else live_keys)
+    if grow_start is None:
+        grow_start = 0.8 * max_load
+    cfg = ServeConfig(depth, max_batch, max_load, table.size() if live_keys is None else live_keys, grow_start)
     st = ServeStats()
     rc = lib().hive_serve_run(table.handle, ctypes.byref(cfg), types.ctypes.data, keys.ctypes.data, vals.ctypes.data,
                               arrival.ctypes.data, n, out_v.ctypes.data, out_s.ctypes.data, done.ctypes.data,

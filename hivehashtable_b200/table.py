@@ -90,6 +90,7 @@ ABI = [
     ("hive_apply_batches", _I32, [_P, _P, _P, _P, _P, _U32, _U64, _P, _P, _U32, _I32, _I32, _P]),
     ("hive_size", _I32, [_P, ctypes.POINTER(_U64), _P]),
     ("hive_dump", _I32, [_P, _P, _U64, ctypes.POINTER(_U64), _P]),
+    ("hive_load", _I32, [_P, _P, _U64, ctypes.POINTER(_U64), _P]),
     ("hive_resize", _I32, [_P, _U64, _P]),
     ("hive_bucket_of", _I32, [_P, _P, _U64, _P, _P, _P]),
     ("hive_get_info", _I32, [_P, ctypes.POINTER(Info)]),
@@ -346,6 +347,67 @@ class HiveHashTable:
         vals = (a >> 32).astype(np.uint32)
         order = np.argsort(keys, kind="stable")
         return keys[order], vals[order]
+
+    def dump_packed(self, stream=None) -> torch.Tensor:
+        """All entries as one device int64 tensor of packed (value << 32) | key words, unordered:
+        the format load() takes back."""
+        cap = self.size(stream)
+        kv = torch.empty(max(cap, 1), dtype=torch.int64, device=self.device)
+        n = ctypes.c_uint64()
+        _check(self._lib.hive_dump(self._h, _ptr(kv), cap, ctypes.byref(n), self._stream(stream)),
+               "hive_dump")
+        if n.value != cap:
+            raise HiveError(1, f"hive_dump: table changed size during dump ({n.value} != {cap})")
+        return kv[:cap]
+
+    def load(self, keys, values=None, stream=None) -> None:
+        """Replace the contents with the given entries (unique keys): `keys` alone is a packed
+        int64 tensor as dump_packed() returns; with `values`, two uint32 arrays.  Grows the table
+        to the next full level when the entries exceed load factor 0.9 of its unsplit level.  Raises HiveError(6) if any entry found no room
+        (or has key 0); the table then holds the others."""
+        if values is None:
+            kv = keys.to(self.device).contiguous() if isinstance(keys, torch.Tensor) else \
+                torch.from_numpy(np.ascontiguousarray(np.asarray(keys, dtype=np.uint64)).view(np.int64)).to(self.device)
+            if kv.dtype != torch.int64 or kv.dim() != 1:
+                raise ValueError("packed entries must be a 1-D int64 tensor")
+        else:
+            k = as_device_u32(keys, self.device).to(torch.int64) & 0xFFFFFFFF
+            v = as_device_u32(values, self.device).to(torch.int64)
+            if k.numel() != v.numel():
+                raise ValueError("keys and values differ in length")
+            kv = (v << 32) | k
+        bad = ctypes.c_uint64()
+        rc = self._lib.hive_load(self._h, _ptr(kv), kv.numel(), ctypes.byref(bad), self._stream(stream))
+        if rc == 6 and bad.value:
+            raise HiveError(6, f"hive_load: {bad.value} of {kv.numel()} entries not placed")
+        _check(rc, "hive_load")
+
+    def save(self, path, stream=None) -> None:
+        """Write a checkpoint file (numpy .npz): the policy, the capacity and every entry."""
+        kv = self.dump_packed(stream).cpu().numpy().view(np.uint64)
+        inf = self.info()
+        with open(path, "wb") as f:
+            np.savez(f, kv=kv, policy=np.array(self.policy), base_buckets=np.uint64(inf["base_buckets"]),
+                     num_buckets=np.uint64(inf["num_buckets"]), max_buckets=np.uint64(inf["max_buckets"]),
+                     max_evictions=np.uint32(inf["max_evictions"]))
+
+    @classmethod
+    def restore(cls, path, device=None, stream=None) -> "HiveHashTable":
+        """A new table from a checkpoint file written by save(): the saved policy, eviction bound and
+        bucket geometry (creation size, then grown to the saved size), holding the saved entries."""
+        with np.load(path) as z:
+            kv, policy = z["kv"], str(z["policy"])
+            base, nb, mx = int(z["base_buckets"]), int(z["num_buckets"]), int(z["max_buckets"])
+            ev = int(z["max_evictions"])
+        t = cls(base * 8, policy, max_evictions=ev, max_capacity=mx * 8, device=device)
+        try:
+            if nb > base:
+                t.resize(nb * 8, stream)
+            t.load(kv, stream=stream)
+        except Exception:
+            t.close()
+            raise
+        return t
 
     def clear(self, stream=None) -> None:
         _check(self._lib.hive_clear(self._h, self._stream(stream)), "hive_clear")

@@ -36,7 +36,7 @@ extern "C" {
 #define HIVE_ERR_OOM 3           /* device allocation failed                                   */
 #define HIVE_ERR_LOCK_TIMEOUT 4  /* a bucket-lock wait expired inside a kernel (sticky)        */
 #define HIVE_ERR_RETRY_LIMIT 5   /* a CAS retry budget ran out inside a kernel (sticky)        */
-#define HIVE_ERR_CAPACITY 6      /* resize target beyond the reserved capacity                 */
+#define HIVE_ERR_CAPACITY 6      /* resize refused, or hive_load entries that found no room    */
 #define HIVE_ERR_NO_DEVICE 7     /* no CUDA device / the library was not built for it         */
 
 /* ---- hash policies (reference include/HashPolicies.cuh:10-17, :29-36) ------------------------ */
@@ -214,6 +214,15 @@ int hive_size(hive_table* t, uint64_t* n_out, void* stream);
  * counterpart: the reference has no way to read its table back (its compact_stash_kernel,
  * include/hive_stash_table.cuh:33-64, does this for the stash only). */
 int hive_dump(hive_table* t, uint64_t* kv, uint64_t cap, uint64_t* n_out, void* stream);
+
+/* Restore a table from n packed entries in the device array kv, in hive_dump's format and any
+ * order: empties the table (keeping its current number of buckets), grows it to the next full
+ * linear-hashing level when n exceeds load factor 0.9 of the slots of its unsplit level
+ * (8 * n_lo, n_lo = base_buckets << level), and inserts every entry.  Keys must be unique, as a dump's are (a repeated key keeps
+ * one of its values).  *n_unplaced (may be NULL) = entries not placed: key 0, or no room left;
+ * the call then returns HIVE_ERR_CAPACITY and the table holds the others.  Synchronises `stream`.
+ * No reference counterpart: the reference keeps no checkpoint of its table. */
+int hive_load(hive_table* t, const uint64_t* kv, uint64_t n, uint64_t* n_unplaced, void* stream);
 
 /* Grow or shrink to ceil(target_slots / 8) buckets by linear-hashing split/merge, stream-ordered
  * between other calls (synchronises `stream`).  Growth beyond the reserved capacity reallocates.

@@ -459,6 +459,77 @@ def test_resize_grow_and_shrink(cuda, policy):
         t.check()
 
 
+@pytest.mark.parametrize("policy", POLICIES)
+def test_dump_load_and_checkpoint(cuda, policy, tmp_path):
+    """dump -> load into a smaller table (which grows) and save -> restore give the replay's
+    key->value set; a restored table keeps the saved geometry, split pointer included."""
+    keys, absent, st = oracle.gen_keys(29, 150_000, 20_000)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(1 << 15, policy, max_capacity=1 << 19) as a:
+        a.resize(1 << 18)
+        _insert_and_check(a, m, keys, vals)
+        gone = keys[::3]
+        np.testing.assert_array_equal(_np(a.erase(gone)), m.erase(gone))
+        a.resize((1 << 18) + 8 * 777)  # split pointer mid-level
+        _assert_same_set(a, m)
+        kv = a.dump_packed()
+        assert kv.numel() == len(m)
+        look, _ = oracle.lookup_set(keys, absent, 30_000, 30_000, st)
+        with HiveHashTable(1 << 14, policy) as b:
+            b.insert(absent[:5000], absent[:5000])  # replaced by the load
+            b.load(kv)
+            assert b.info()["capacity_slots"] >= len(m) / 0.9
+            _assert_same_set(b, m)
+            _find_and_check(b, m, look)
+            # the unpacked form, into the table's existing size
+            k, v = a.dump()
+            b.load(k, v)
+            _assert_same_set(b, m)
+            b.check()
+        path = tmp_path / "table.npz"
+        a.save(path)
+        with HiveHashTable.restore(path) as c:
+            ia, ic = a.info(), c.info()
+            for f in ("num_buckets", "base_buckets", "level", "split", "max_buckets", "max_evictions", "policy"):
+                assert ia[f] == ic[f], f
+            _assert_same_set(c, m)
+            _find_and_check(c, m, look)
+            # the restored table takes further batches like the original
+            more = absent[:10_000]
+            _insert_and_check(c, m, more, oracle.values_for(more))
+            _assert_same_set(c, m)
+            c.check()
+
+
+def test_load_edge_cases(cuda):
+    """Empty input, key 0 (reported as unplaced), and a load across two internal chunks."""
+    with HiveHashTable(1 << 16) as t:
+        t.insert(np.arange(1, 1001, dtype=np.uint32), np.arange(1, 1001, dtype=np.uint32))
+        t.load(torch.empty(0, dtype=torch.int64, device="cuda"))
+        assert t.size() == 0 and t.info()["capacity_slots"] == 1 << 16
+        # key 0 is not storable: reported, the rest placed
+        k = np.array([0, 5, 6, 7], dtype=np.uint32)
+        with pytest.raises(HiveError) as e:
+            t.load(k, k + np.uint32(1))
+        assert e.value.code == 6 and "1 of 4" in str(e.value)
+        gk, gv = t.dump()
+        np.testing.assert_array_equal(gk, [5, 6, 7])
+        np.testing.assert_array_equal(gv, [6, 7, 8])
+    # 2^22 + 4321 entries: two chunks of the load's staging, and growth from 2^16 slots
+    n = (1 << 22) + 4321
+    keys, _, _ = oracle.gen_keys(31, n, 0)
+    vals = oracle.values_for(keys)
+    with HiveHashTable(1 << 16, max_capacity=1 << 24) as t:
+        t.load(keys, vals)
+        assert t.size() == n and t.info()["capacity_slots"] >= n / 0.9
+        gk, gv = t.dump()
+        order = np.argsort(keys)
+        np.testing.assert_array_equal(gk, keys[order])
+        np.testing.assert_array_equal(gv, vals[order])
+        assert t.verify() == {"tag_mismatch": 0, "misplaced": 0, "duplicate": 0, "stale_tag": 0}
+
+
 def test_bucket_choice_matches_oracle(cuda):
     keys = np.random.RandomState(0).randint(0, 2**32, size=100_000, dtype=np.uint64).astype(np.uint32)
     for policy, pid in (("Default2Hash", 0), ("MurmurCityHash", 1)):

@@ -68,3 +68,41 @@ def test_growth_under_inserts(cuda):
         np.testing.assert_array_equal(r.out_vals, exp_v)
         assert r.stats["resizes"] >= 1 and t.info()["capacity_slots"] > (1 << 13)
         assert t.size() == len(m)
+
+
+@pytest.mark.parametrize("grow_start", [0.0, 0.6])
+def test_incremental_growth_matches_replay(cuda, grow_start):
+    """Growth in bounded split steps between batches (no drain) and growth at once after a drain
+    both keep every result equal to the arrival-order replay; the incremental run finishes its
+    doublings before the load reaches max_load, so it never drains."""
+    w = ServedWorkload(37, 1 << 14, 1 << 18, "D")
+    with HiveHashTable(1 << 15, max_capacity=1 << 18) as t:
+        t.insert(w.preload_keys, w.preload_vals)
+        r = serve(t, w.types, w.keys, w.vals, np.zeros(w.keys.size), depth=4, max_batch=512, max_load=0.85,
+                  grow_start=grow_start)
+        exp_s, exp_v, m = _expected(w, w.types, w.keys, w.vals)
+        np.testing.assert_array_equal(r.out_status, exp_s)
+        np.testing.assert_array_equal(r.out_vals, exp_v)
+        gk, gv = t.dump()
+        ok, ov = m.dump()
+        np.testing.assert_array_equal(gk, ok)
+        np.testing.assert_array_equal(gv, ov)
+        assert r.stats["resizes"] >= 1 and t.info()["capacity_slots"] > (1 << 15)
+        if grow_start:
+            assert r.stats["grow_steps"] > r.stats["resizes"] and r.stats["drains"] == 0, r.stats
+        else:
+            assert r.stats["grow_steps"] == 0 and r.stats["drains"] == r.stats["resizes"], r.stats
+        v = t.verify()
+        assert v["tag_mismatch"] == v["misplaced"] == v["duplicate"] == 0, v
+        t.check()
+
+
+def test_grow_start_bounds(cuda):
+    from hivehashtable_b200 import HiveError
+    w = ServedWorkload(41, 1 << 10, 1 << 10, "A")
+    with HiveHashTable(1 << 12) as t:
+        t.insert(w.preload_keys, w.preload_vals)
+        for gs, ml in ((0.9, 0.9), (-0.1, 0.9), (0.5, 0.0)):
+            with pytest.raises(HiveError) as e:
+                serve(t, w.types, w.keys, w.vals, np.zeros(w.keys.size), max_load=ml, grow_start=gs)
+            assert e.value.code == 1
