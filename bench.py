@@ -45,7 +45,7 @@ BYTES_LOOKUP_ABSENT = 140.0
 # at this workload (2^26 slots, LF 0.9, Default2Hash): the insert's three launches (first pass,
 # deferred pass, fingerprint rebuild) and k_find; profiles/bulk_insert_lookup_2p26_dram_traffic.txt.
 # A measurement of this build: re-capture after a change to either kernel.
-TRAFFIC_PER_OP = {"insert": 186.1, "lookup": 99.9}
+TRAFFIC_PER_OP = {"insert": 185.6, "lookup": 99.6}
 
 
 def parse_args():
@@ -85,31 +85,64 @@ def load_peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+    """Samples the GPU's SM clock and clock-event (throttle) reasons while the timed region runs:
+    through NVML every 5 ms (read-only queries), else through nvidia-smi every 200 ms."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
-        self.rows = []
+        self.rows = []          # (sm_mhz, max_mhz, set of active reason names)
+        self.source = None
         self._stop = threading.Event()
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
+    def _nvml(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(self.index)
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0")
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        bits = [pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap]
+        mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+        def sample():
+            sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+            r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+            return float(sm), float(mx), {n for n, b in zip(self.NAMES, bits) if r & b}
+        return sample
+
+    def _smi(self):
+        def sample():
+            out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+            c = [x.strip() for x in out.stdout.strip().splitlines()[0].split(",")]
+            return float(c[1]), float(c[2]), {n for i, n in enumerate(self.NAMES) if c[5 + i] == "Active"}
+        return sample
+
+    def _run(self, sample, period):
+        while True:
             try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for ln in out.stdout.strip().splitlines():
-                    self.rows.append([c.strip() for c in ln.split(",")])
+                self.rows.append(sample())
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            if self._stop.wait(period):
+                break
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        try:
+            sample, period, self.source = self._nvml(), 0.005, "nvml"
+            sample()
+        except Exception:
+            sample, period, self.source = self._smi(), 0.2, "nvidia-smi"
+        self._t = threading.Thread(target=self._run, args=(sample, period), daemon=True)
         self._t.start()
         return self
 
@@ -119,12 +152,11 @@ class ClockSampler:
             self._t.join(timeout=10)
 
     def summary(self):
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(sm)}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted(set().union(*[r[2] for r in self.rows])) if self.rows else []
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(r[1] for r in self.rows) if self.rows else None,
+                "reasons": reasons, "samples": len(sm), "source": self.source}
 
 
 def random_bucket_ceiling(dev, table_bytes):
@@ -358,8 +390,8 @@ def run_resize(args, dev):
     """Growth and shrink (seed 13): a 2^20-slot table takes 2^27 unique keys in 128 chunks of
     2^20 inserts, each followed by 2^17 lookups of inserted keys, doubling (linear-hashing splits)
     before a chunk would pass LF 0.85; then 75 % of the keys are deleted in random order in chunks of
-    2^20, shrinking to LF 0.75 whenever the load falls below 0.25.  Device time of each phase with
-    its resizes included."""
+    2^20, shrinking whenever the load falls below 0.25 by whole levels (halving while the keys fit
+    the half at LF 0.75).  Device time of each phase with its resizes included."""
     import numpy as np
     import torch
     from hivehashtable_b200 import HiveHashTable, as_device_u32
@@ -414,8 +446,13 @@ def run_resize(args, dev):
             live = n - min(c + chunk, gone.numel())
             cap = t.info()["capacity_slots"]
             if live < 0.25 * cap:
-                t.resize(max(int(live / 0.75) // 8 * 8, 1 << 20))
-                shrinks += 1
+                # whole levels: halve while the entries fit the half at LF 0.75
+                tgt = cap
+                while tgt // 2 >= 1 << 20 and live <= 0.75 * (tgt // 2):
+                    tgt //= 2
+                if tgt != cap:
+                    t.resize(tgt)
+                    shrinks += 1
         b.record(stream)
         torch.cuda.synchronize()
         del_ms = a.elapsed_time(b)

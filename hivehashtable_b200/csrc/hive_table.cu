@@ -1681,11 +1681,15 @@ int hive_resize(hive_table* h, uint64_t target_slots, void* stream) {
     if (target < h->n0) target = h->n0;  // never below the creation size (level 0)
     if (target < num_buckets(h)) {
         // A shrink is refused (table unchanged) unless the live entries fit the smaller table at
-        // load factor <= kMaxShrinkLoad, so the merge's re-inserts cannot run out of room.
+        // load factor <= kMaxShrinkLoad, so the merge's re-inserts cannot run out of room.  The
+        // load counted is that of the target's unsplit level: mid-level, a bucket not yet split
+        // takes keys of 1/n_lo of the hash space, twice a split bucket's share.
         uint64_t live = 0;
         int rc = hive_size(h, &live, stream);
         if (rc) return rc;
-        if ((double)live > kMaxShrinkLoad * (double)(target * hive::kSlots)) return HIVE_ERR_CAPACITY;
+        uint64_t lvl = h->n0;
+        while (lvl * 2 <= target) lvl *= 2;
+        if ((double)live > kMaxShrinkLoad * (double)(lvl * hive::kSlots)) return HIVE_ERR_CAPACITY;
     }
     int rc = grow_capacity(h, target, s);
     if (rc) return rc;

@@ -227,7 +227,8 @@ int hive_load(hive_table* t, const uint64_t* kv, uint64_t n, uint64_t* n_unplace
 /* Grow or shrink to ceil(target_slots / 8) buckets by linear-hashing split/merge, stream-ordered
  * between other calls (synchronises `stream`).  Growth beyond the reserved capacity reallocates.
  * A shrink stops at the creation size and is refused with HIVE_ERR_CAPACITY (table unchanged)
- * when the live entries would exceed load factor 0.9 of the target.
+ * when the live entries would exceed load factor 0.9 of the slots of the target's unsplit level
+ * (8 * n_lo: mid-level, those buckets take twice a split bucket's share of the keys).
  * Replaces hive_hash_grow / hive_hash_shrink (include/hive_hash_resize.cuh:138-215, :340-420). */
 int hive_resize(hive_table* t, uint64_t target_slots, void* stream);
 

@@ -449,6 +449,11 @@ def test_resize_grow_and_shrink(cuda, policy):
         with pytest.raises(HiveError) as e:
             t.resize(1 << 10)
         assert e.value.code == 6 and t.info()["capacity_slots"] == 1 << 15
+        # 24,000 slots would hold them at LF 0.83, but mid-level its 2^14 unsplit slots would take
+        # them at 1.22: refused as well
+        with pytest.raises(HiveError) as e:
+            t.resize(24_000)
+        assert e.value.code == 6 and t.info()["capacity_slots"] == 1 << 15
         _assert_same_set(t, m)
         more = keys[100_000: 110_000]
         np.testing.assert_array_equal(_np(t.erase(more)), m.erase(more))
