@@ -517,7 +517,9 @@ __device__ __forceinline__ bool find_tagged(const Table& t, uint32_t b, u64 T, u
 
 // The slots are read only where a fingerprint matches; the stash has no tags and is read whole
 // when its flag is set.  Read-only kernels (nothing changes during the launch) read both tag
-// words up front, two independent L2 reads.  Otherwise H1's tags are read only after H0 missed:
+// words up front, two independent L2 reads (reading H1's only after H0 missed saves tag-word
+// accesses but was measured slower, even at 2^23 buckets where the words outgrow what L2 keeps).
+// Otherwise H1's tags are read only after H0 missed:
 // an eviction writes the victim (and its fingerprint) to H1 before removing it from H0, so
 // reading H0 then H1 in that order always finds it.
 template <int P, bool kReadOnly>

@@ -150,12 +150,19 @@ struct Defer {
     uint32_t* q;
     u64* n;
     uint32_t permute = 0;
+    // Bulk inserts: the deferred op's packed (value << 32) | key beside its index, so the second
+    // pass reads its ops from the queue sequentially instead of gathering them from the batch;
+    // the first pass then also writes HIVE_ST_INSERTED as the deferred op's provisional status
+    // and the second pass writes only statuses that differ from it (an eviction, the common
+    // outcome, leaves the byte alone: a scattered 1-byte write costs a DRAM read and write).
+    u64* kv = nullptr;
 };
 
 // The second pass visits queue position defer_slot(j, cnt) at step j.  In submission order the
 // queue is already in random bucket order and is visited in order: consecutive queue entries hold
 // increasing op indices, so the keys, values and statuses they name are read and written nearly
-// sequentially (a permuted visit made them random accesses, the pass's largest cost).  A
+// sequentially (a permuted visit made them random accesses, the pass's largest cost), and with
+// Defer::kv the keys and values come from the queue itself.  A
 // region-ordered batch's queue is in bucket order; it is visited through a bijection of [0, cnt)
 // (multiplication by a prime larger than any queue) so that its deferred ops are finished in an
 // order unrelated to their buckets: finished in bucket order, the last buckets' overflow would
@@ -165,9 +172,9 @@ __device__ __forceinline__ u64 defer_slot(u64 j, u64 cnt, uint32_t permute) {
     return permute ? (j * (4294967311ull % cnt)) % cnt : j;
 }
 
-// Appends index i for every lane whose st is kStDefer, one atomic per warp.  Every lane of the
-// warp must call it.
-__device__ __forceinline__ void defer_push(const Defer& d, bool deferred, uint64_t i) {
+// Appends index i (and, with Defer::kv, the op's packed kv) for every lane whose st is kStDefer,
+// one atomic per warp.  Every lane of the warp must call it.
+__device__ __forceinline__ void defer_push(const Defer& d, bool deferred, uint64_t i, u64 kv = 0) {
     const unsigned m = __ballot_sync(0xffffffffu, deferred);
     if (!m) return;
     const unsigned lane = threadIdx.x & 31;
@@ -175,7 +182,11 @@ __device__ __forceinline__ void defer_push(const Defer& d, bool deferred, uint64
     u64 base = 0;
     if ((int)lane == leader) base = atomicAdd(d.n, (u64)__popc(m));
     base = __shfl_sync(0xffffffffu, base, leader);
-    if (deferred) d.q[base + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
+    if (deferred) {
+        const u64 pos = base + __popc(m & ((1u << lane) - 1u));
+        d.q[pos] = (uint32_t)i;
+        if (d.kv) d.kv[pos] = kv;
+    }
 }
 
 // First pass (kDefer) or the whole protocol in one pass (!kDefer, batches too large to queue)
@@ -189,21 +200,48 @@ __global__ void __launch_bounds__(kBlock, (kDefer && hive::mode_base(kMode) == h
     const bool active = i < hi;
     uint8_t st = hive::kStFail;
     if (active) st = hive::insert_one<P, kDefer, kMode>(t, __ldcs(keys + i), __ldcs(vals + i));
-    if (kDefer) defer_push(d, st == hive::kStDefer, i);
-    if (active && st != hive::kStDefer && status) __stcs(status + i, st);
+    // a deferred op's key and value are read again (L2 hits: the lines were just streamed in)
+    // rather than kept live across the insert
+    u64 kv = 0;
+    if (kDefer && st == hive::kStDefer && d.kv) kv = hive::pack(__ldcg(keys + i), __ldcg(vals + i));
+    if (kDefer) defer_push(d, st == hive::kStDefer, i, kv);
+    // a deferred op's provisional status (Defer::kv) is kStInserted
+    if (active && status && (st != hive::kStDefer || d.kv)) __stcs(status + i, st == hive::kStDefer ? hive::kStInserted : st);
 }
 
-// Second pass: the deferred inserts, grid-stride over the queue.
-template <int P>
+// Second pass: the deferred inserts, grid-stride over the queue.  kKV: the queue carries the ops'
+// packed kv (Defer::kv) and the statuses are provisionally kStInserted; else the ops are gathered
+// from the batch by index and every status is written.
+template <int P, bool kKV>
 __global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, const uint32_t* __restrict__ keys,
                                                             const uint32_t* __restrict__ vals,
                                                             uint8_t* __restrict__ status, Defer d) {
     const u64 cnt = *d.n;
-    for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
-        const uint32_t i = d.q[defer_slot(j, cnt, d.permute)];
-        const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals[i]);
-        if (status) status[i] = st;
+    const u64 stride = (u64)gridDim.x * kBlock;
+    u64 j = (u64)blockIdx.x * kBlock + threadIdx.x;
+    if constexpr (kKV) {
+        // (An L2 prefetch of the next op's buckets and lock word while this op runs was measured
+        // slower: the lines were evicted before use and the pass's DRAM traffic grew by a third.)
+        for (; j < cnt; j += stride) {
+            const u64 q = defer_slot(j, cnt, d.permute);
+            const u64 e = __ldcs(d.kv + q);
+            const uint8_t st = hive::insert_deferred_one<P>(t, hive::key_of(e), hive::val_of(e));
+            if (status && st != hive::kStInserted) status[__ldcs(d.q + q)] = st;
+        }
+    } else {
+        for (; j < cnt; j += stride) {
+            const uint32_t i = d.q[defer_slot(j, cnt, d.permute)];
+            const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals[i]);
+            if (status) status[i] = st;
+        }
     }
+}
+
+template <int P>
+void launch_second_pass(unsigned grid, cudaStream_t s, const hive::Table& t, const uint32_t* keys,
+                        const uint32_t* vals, uint8_t* status, const Defer& d) {
+    if (d.kv) k_insert_deferred<P, true><<<grid, kBlock, 0, s>>>(t, keys, vals, status, d);
+    else k_insert_deferred<P, false><<<grid, kBlock, 0, s>>>(t, keys, vals, status, d);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -846,7 +884,8 @@ int table_view(hive_table* h, cudaStream_t s, hive::Table* tv) {
 
 // The deferred-op queue for a batch of n ops; grows (synchronously) to the largest batch seen.
 // Batches of 2^32 ops or more run without deferral.
-int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d) {
+// The queue of a batch of n ops: n indices and, for bulk inserts (with_kv), n packed kv words.
+int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d, bool with_kv = false) {
     *d = Defer{nullptr, h->scratch + 1};
     if (n > 0xFFFFFFFFull) return HIVE_OK;
     if (n > h->defer_cap) {
@@ -854,12 +893,13 @@ int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d) {
         if (h->defer_q) cudaFree(h->defer_q);
         h->defer_q = nullptr;
         h->defer_cap = 0;
-        cudaError_t e = cudaMalloc(&h->defer_q, (size_t)n * 4);
+        cudaError_t e = cudaMalloc(&h->defer_q, align256((size_t)n * 4) + (size_t)n * 8);
         if (e != cudaSuccess) return cuda_fail(e);
         h->defer_cap = n;
     }
     HIVE_CUDA(cudaMemsetAsync(h->scratch + 1, 0, 8, s));
     d->q = h->defer_q;
+    if (with_kv) d->kv = (u64*)((char*)h->defer_q + align256((size_t)h->defer_cap * 4));
     return HIVE_OK;
 }
 
@@ -1157,6 +1197,13 @@ int hive_clear(hive_table* h, void* stream) {
     return HIVE_OK;
 }
 
+// Calls the host-side launcher fn<P>(...) for the table's policy.
+#define HIVE_DISPATCH_FN(fn, ...)                                                          \
+    do {                                                                                   \
+        if (h->policy == HIVE_POLICY_MURMURCITYHASH) fn<1>(__VA_ARGS__);                    \
+        else fn<0>(__VA_ARGS__);                                                           \
+    } while (0)
+
 #define HIVE_DISPATCH(kern, grid, block, stream, ...)                                      \
     do {                                                                                   \
         if (h->policy == HIVE_POLICY_MURMURCITYHASH) kern<1><<<grid, block, 0, stream>>>(__VA_ARGS__); \
@@ -1257,7 +1304,7 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     Defer d;
-    int rc = prepare_defer(h, n, s, &d);
+    int rc = prepare_defer(h, n, s, &d, true);
     if (rc) return rc;
     hive::Table tt;
     bool untag;
@@ -1277,20 +1324,20 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
             const uint64_t lo = ((uint64_t)k * n + nsub - 1) / nsub, hi = ((uint64_t)(k + 1) * n + nsub - 1) / nsub;
             const uint64_t m = hi - lo;
             if (!m) continue;
-            if (k && (rc = prepare_defer(h, m, s, &d))) return rc;
+            if (k && (rc = prepare_defer(h, m, s, &d, true))) return rc;
             d.permute = 1;  // the queue is in bucket order
             uint8_t* rst = status ? r.rst + lo : nullptr;
             launch_first_pass(h, tr, d, 0, m, s, r.rkeys + lo, r.rvals + lo, rst, !single);
             if (d.q)
-                HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, m), kBlock, s, tr, r.rkeys + lo, r.rvals + lo, rst,
-                              d);
+                HIVE_DISPATCH_FN(launch_second_pass, second_pass_grid(h, m), s, tr, r.rkeys + lo, r.rvals + lo,
+                                 rst, d);
         }
         if (untag) retag(h, s);
         if (status) k_unpermute_u8<<<grid_for(n), kBlock, 0, s>>>(r.ridx, r.rst, n, status);
         return launch_check();
     }
     launch_first_pass(h, tt, d, 0, n, s, keys, values, status, false);
-    if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, tt, keys, values, status, d);
+    if (d.q) HIVE_DISPATCH_FN(launch_second_pass, second_pass_grid(h, n), s, tt, keys, values, status, d);
     if (untag) retag(h, s);
     return launch_check();
 }
@@ -1346,7 +1393,7 @@ int hive_insert_noalloc(hive_table* h, const uint32_t* keys, const uint32_t* val
     bool untag;
     if ((rc = insert_view(h, n, s, &tt, &untag))) return rc;
     launch_first_pass(h, tt, d, 0, n, s, keys, values, status, false);
-    HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, tt, keys, values, status, d);
+    HIVE_DISPATCH_FN(launch_second_pass, second_pass_grid(h, n), s, tt, keys, values, status, d);
     if (untag) retag(h, s);
     return launch_check();
 }
@@ -1435,7 +1482,7 @@ int hive_insert_host(hive_table* h, const uint32_t* keys, const uint32_t* values
     Staging st;
     Defer d;
     int rc;
-    if ((rc = prepare_pipe(h, n, &st)) || (rc = prepare_defer(h, n, s, &d))) return rc;
+    if ((rc = prepare_pipe(h, n, &st)) || (rc = prepare_defer(h, n, s, &d, true))) return rc;
     HIVE_CUDA(cudaStreamWaitEvent(h->pipe_h2d, h->ev_ins_free, 0));
     uint8_t* dst = status ? st.ist : nullptr;
     hive::Table tt;
@@ -1449,7 +1496,7 @@ int hive_insert_host(hive_table* h, const uint32_t* keys, const uint32_t* values
         // first pass of this chunk; its deferred ops join the batch's one queue
         launch_first_pass(h, tt, d, lo, lo + m, s, st.ik, st.iv, dst, false);
     }
-    if (d.q) HIVE_DISPATCH(k_insert_deferred, second_pass_grid(h, n), kBlock, s, tt, st.ik, st.iv, dst, d);
+    if (d.q) HIVE_DISPATCH_FN(launch_second_pass, second_pass_grid(h, n), s, tt, st.ik, st.iv, dst, d);
     if (untag) retag(h, s);
     if (status) {
         HIVE_CUDA(order(h->ev_out, s, h->pipe_d2h));

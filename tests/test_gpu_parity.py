@@ -264,6 +264,27 @@ def test_tuning_bounds(cuda):
         _assert_same_set(t, m)
 
 
+@pytest.mark.parametrize("policy", POLICIES)
+def test_read_only_lookup_paths(cuda, policy):
+    """The read-only lookup path answers as the replay through hive_find, the host-buffer path and
+    lookup-only reference records."""
+    n = 300_000
+    keys, absent, st = oracle.gen_keys(43, n, n)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(int(n / 0.9), policy) as t:
+        _insert_and_check(t, m, keys, vals)
+        look, _ = oracle.lookup_set(keys, absent, n // 2, n // 2, st)
+        _find_and_check(t, m, look)
+        hv, hf = t.find_host(look)
+        ev, ef = m.find(look)
+        np.testing.assert_array_equal(np.asarray(hf).astype(np.uint8), ef)
+        np.testing.assert_array_equal(np.asarray(hv).view(np.uint32), ev)
+        ops = torch.from_numpy(np.stack([np.full(look.size, OP_LOOKUP, np.int64), look.astype(np.int64)], 1))
+        res = _np(t.apply_reference_ops(ops, hints=2))
+        np.testing.assert_array_equal(res, ef.astype(np.int64))
+
+
 def test_reference_record_path(cuda):
     """16-byte Operation records, value = key + 1, uint64 0/1 results (the reference's kernel
     contract, include/hive_kernels.cuh:119-266)."""
