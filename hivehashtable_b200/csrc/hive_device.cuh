@@ -662,93 +662,103 @@ __device__ __forceinline__ bool resolve_duplicate(const Table& t, uint32_t b, ui
 
 enum { kEvPlaced = 1, kEvRetry = 2, kEvNone = 0 };
 
+// Victims are considered in groups of kEvictGroup slots: a group's candidates (slots j < limit,
+// the reference's kick % 8 order, whose key lives in its own H0 = b0 and whose H1 is another
+// bucket) are hashed and their H1 full bits read in one round of independent L2 reads, then the
+// open ones are tried in slot order; the next group is hashed only if none of them took a victim.
+// The order of attempts is that of all open candidates in slot order, but a first group that
+// places the victim (the common case) spares the other group's hashing, most of this path's
+// instructions.
+constexpr int kEvictGroup = 4;
+
 template <int P>
 __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket& B0, uint32_t b0, u64 kv) {
     const int limit = t.max_evictions < (uint32_t)kSlots ? (int)t.max_evictions : kSlots;
-    // Candidate victims: slots j < limit (the reference's kick % 8 order) whose key lives in its
-    // own H0 (= b0) and whose H1 is another bucket.  A slot that freed up is taken directly.
-    uint32_t alts[kSlots];
-    uint32_t cand = 0;
+#pragma unroll 1
+    for (int g = 0; g < limit; g += kEvictGroup) {
+        uint32_t alts[kEvictGroup];
+        uint32_t cand = 0;
 #pragma unroll
-    for (int j = 0; j < kSlots; ++j) {
-        alts[j] = b0;
-        if (j >= limit) continue;
-        const u64 vkv = B0.s[j];
-        if (vkv == 0ull) {
-            if (cas64(B0p + j, 0ull, kv) != 0ull) return kEvRetry;
-            tag_set(t, b0, j, tag_of(key_of(kv)));
-            return kEvPlaced;
-        }
-        const uint32_t vk = key_of(vkv);
-        if (bucket_addr(t, Policy<P>::h0(vk)) != b0) continue;  // victim lives in its H1
-        const uint32_t alt = bucket_addr(t, Policy<P>::h1(vk));
-        if (alt == b0) continue;
-        alts[j] = alt;
-        cand |= 1u << j;
-    }
-    // One round of independent L2 reads of the candidates' full bits instead of a chain of
-    // bucket reads; only buckets not known to be full are read.
-    uint32_t open = 0;
-#pragma unroll
-    for (int j = 0; j < kSlots; ++j)
-        if ((cand >> j) & 1u)
-            if (!((__ldcg(t.full_bits + (alts[j] >> 5)) >> (alts[j] & 31)) & 1u)) open |= 1u << j;
-    while (open) {
-        const int j = __ffs(open) - 1;
-        open &= open - 1;
-        u64 vkv = slot_at(B0, j);
-        const uint32_t vk = key_of(vkv);
-        uint32_t alt = alts[0];
-#pragma unroll
-        for (int q = 1; q < kSlots; ++q)
-            if (q == j) alt = alts[q];
-        u64* Ap = t.slots + (size_t)alt * kSlots;
-        Bucket A;
-        load_bucket(Ap, A);
-        const uint32_t e = empty_mask(A);
-        if (!e) {
-            mark_full(t, alt);
-            continue;
-        }
-        const int d = __ffs(e) - 1;
-        if (cas64(Ap + d, 0ull, vkv) != 0ull) continue;  // lost the free slot; next victim
-        if (__popc(e) == 1) mark_full(t, alt);
-        // The copy's fingerprint is in place before H0's slot changes (tag_set completes).
-        tag_set(t, alt, d, tag_of(vk));
-        // The victim is now visible in both H0 slot j and H1 slot d.
-        const uint32_t f = tag_of(key_of(kv));
-        for (int r = 0; r < kRetryLimit; ++r) {
-            u64 obs = cas64(B0p + j, vkv, kv);
-            if (obs == vkv) {
-                tag_set(t, b0, j, f);
-                count(t, kCtrEvictions);
+        for (int q = 0; q < kEvictGroup; ++q) {
+            const int j = g + q;
+            alts[q] = b0;
+            if (j >= limit) continue;
+            const u64 vkv = slot_at(B0, j);
+            if (vkv == 0ull) {  // a slot that freed up is taken directly
+                if (cas64(B0p + j, 0ull, kv) != 0ull) return kEvRetry;
+                tag_set(t, b0, j, tag_of(key_of(kv)));
                 return kEvPlaced;
             }
-            if (obs == 0ull) {
-                // Victim deleted meanwhile: drop the copy unless it changed, take the free slot.
+            const uint32_t vk = key_of(vkv);
+            if (bucket_addr(t, Policy<P>::h0(vk)) != b0) continue;  // victim lives in its H1
+            const uint32_t alt = bucket_addr(t, Policy<P>::h1(vk));
+            if (alt == b0) continue;
+            alts[q] = alt;
+            cand |= 1u << q;
+        }
+        uint32_t open = 0;
+#pragma unroll
+        for (int q = 0; q < kEvictGroup; ++q)
+            if ((cand >> q) & 1u)
+                if (!((__ldcg(t.full_bits + (alts[q] >> 5)) >> (alts[q] & 31)) & 1u)) open |= 1u << q;
+        while (open) {
+            const int q0 = __ffs(open) - 1;
+            open &= open - 1;
+            const int j = g + q0;
+            u64 vkv = slot_at(B0, j);
+            const uint32_t vk = key_of(vkv);
+            uint32_t alt = alts[0];
+#pragma unroll
+            for (int q = 1; q < kEvictGroup; ++q)
+                if (q == q0) alt = alts[q];
+            u64* Ap = t.slots + (size_t)alt * kSlots;
+            Bucket A;
+            load_bucket(Ap, A);
+            const uint32_t e = empty_mask(A);
+            if (!e) {
+                mark_full(t, alt);
+                continue;
+            }
+            const int d = __ffs(e) - 1;
+            if (cas64(Ap + d, 0ull, vkv) != 0ull) continue;  // lost the free slot; next victim
+            if (__popc(e) == 1) mark_full(t, alt);
+            // The copy's fingerprint is in place before H0's slot changes (tag_set completes).
+            tag_set(t, alt, d, tag_of(vk));
+            // The victim is now visible in both H0 slot j and H1 slot d.
+            const uint32_t f = tag_of(key_of(kv));
+            for (int r = 0; r < kRetryLimit; ++r) {
+                u64 obs = cas64(B0p + j, vkv, kv);
+                if (obs == vkv) {
+                    tag_set(t, b0, j, f);
+                    count(t, kCtrEvictions);
+                    return kEvPlaced;
+                }
+                if (obs == 0ull) {
+                    // Victim deleted meanwhile: drop the copy unless it changed, take the free slot.
+                    if (cas64(Ap + d, vkv, 0ull) == vkv) {
+                        tag_clear(t, alt, d);
+                        mark_not_full(t, alt);
+                    }
+                    if (cas64(B0p + j, 0ull, kv) != 0ull) return kEvRetry;
+                    tag_set(t, b0, j, f);
+                    return kEvPlaced;
+                }
+                if (key_of(obs) == vk) {
+                    // Victim updated meanwhile: carry the new value to the copy, then retry.
+                    if (cas64(Ap + d, vkv, obs) != vkv) return kEvRetry;
+                    vkv = obs;
+                    continue;
+                }
                 if (cas64(Ap + d, vkv, 0ull) == vkv) {
                     tag_clear(t, alt, d);
                     mark_not_full(t, alt);
                 }
-                if (cas64(B0p + j, 0ull, kv) != 0ull) return kEvRetry;
-                tag_set(t, b0, j, f);
-                return kEvPlaced;
+                return kEvRetry;
             }
-            if (key_of(obs) == vk) {
-                // Victim updated meanwhile: carry the new value to the copy, then retry.
-                if (cas64(Ap + d, vkv, obs) != vkv) return kEvRetry;
-                vkv = obs;
-                continue;
-            }
-            if (cas64(Ap + d, vkv, 0ull) == vkv) {
-                tag_clear(t, alt, d);
-                mark_not_full(t, alt);
-            }
+            count(t, kCtrRetryOut);
+            raise_error(t, kErrRetryOut);
             return kEvRetry;
         }
-        count(t, kCtrRetryOut);
-        raise_error(t, kErrRetryOut);
-        return kEvRetry;
     }
     return kEvNone;
 }
