@@ -71,7 +71,8 @@ struct hive_table {
     uint32_t level = 0;
     void* block = nullptr;   // single allocation holding every array
     size_t block_bytes = 0;
-    u64* scratch = nullptr;  // device words: [0] size/dump count, [1] deferred-op count, [2, 6) verify
+    u64* scratch = nullptr;  // device words: [0] size/dump count, [1] deferred-op count, [2, 6) verify,
+                             // [6] third-pass op count
     uint32_t* defer_q = nullptr;  // deferred-op queue (one index per op of the largest batch)
     uint64_t defer_cap = 0;
     void* rbuf = nullptr;         // region-ordering buffers (13 bytes per op of the largest batch)
@@ -120,7 +121,7 @@ Carve carve(uint64_t nb_cap) {
     c.ctr = align256(c.fbits + words * 4);
     c.tags = align256(c.ctr + kCounterBytes);
     c.scratch = align256(c.tags + (size_t)nb_cap * 8);
-    c.total = align256(c.scratch + 48);  // 6 scratch words
+    c.total = align256(c.scratch + 64);  // 8 scratch words
     return c;
 }
 
@@ -156,6 +157,13 @@ struct Defer {
     // and the second pass writes only statuses that differ from it (an eviction, the common
     // outcome, leaves the byte alone: a scattered 1-byte write costs a DRAM read and write).
     u64* kv = nullptr;
+    u64 cap = ~0ull;  // entries the queue holds (a later count may pass it: see k_insert_deferred)
+    // Bulk inserts: where the second pass hands on the ops whose eviction found no victim (their
+    // index, packed kv and count), for a third pass that takes them to the stash.
+    uint32_t* sq = nullptr;
+    u64* skv = nullptr;
+    u64* sn = nullptr;
+    u64 scap = 0;
 };
 
 // The second pass visits queue position defer_slot(j, cnt) at step j.  In submission order the
@@ -211,25 +219,57 @@ __global__ void __launch_bounds__(kBlock, (kDefer && hive::mode_base(kMode) == h
 
 // Second pass: the deferred inserts, grid-stride over the queue.  kKV: the queue carries the ops'
 // packed kv (Defer::kv) and the statuses are provisionally kStInserted; else the ops are gathered
-// from the batch by index and every status is written.
+// from the batch by index and every status is written.  With Defer::sq (and kFlagDeferStash on
+// the view) an op whose eviction found no victim is handed on to that queue for a third pass
+// (this kernel again, over the handed-on ops); one that finds it full is finished here.
 template <int P, bool kKV>
 __global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, const uint32_t* __restrict__ keys,
                                                             const uint32_t* __restrict__ vals,
                                                             uint8_t* __restrict__ status, Defer d) {
-    const u64 cnt = *d.n;
+    const u64 n = *d.n;
+    const u64 cnt = n < d.cap ? n : d.cap;
     const u64 stride = (u64)gridDim.x * kBlock;
-    u64 j = (u64)blockIdx.x * kBlock + threadIdx.x;
     if constexpr (kKV) {
         // (An L2 prefetch of the next op's buckets and lock word while this op runs was measured
         // slower: the lines were evicted before use and the pass's DRAM traffic grew by a third.)
-        for (; j < cnt; j += stride) {
-            const u64 q = defer_slot(j, cnt, d.permute);
-            const u64 e = __ldcs(d.kv + q);
-            const uint8_t st = hive::insert_deferred_one<P>(t, hive::key_of(e), hive::val_of(e));
-            if (status && st != hive::kStInserted) status[__ldcs(d.q + q)] = st;
+        // Warp-uniform trip count: the hand-on is a warp-wide append.  An op that finds the
+        // third-pass queue full runs again at once with the hand-on off (one call site, so the
+        // insert path is inlined once).
+        const unsigned lane = threadIdx.x & 31;
+        hive::Table tv = t;
+        const uint32_t flags0 = t.flags;
+        for (u64 j0 = (u64)blockIdx.x * kBlock + (threadIdx.x & ~31u); j0 < cnt; j0 += stride) {
+            const u64 j = j0 + lane;
+            const bool active = j < cnt;
+            const u64 q = active ? defer_slot(j, cnt, d.permute) : 0;
+            const u64 e = active ? __ldcs(d.kv + q) : 0ull;
+            uint8_t st = hive::kStInserted;
+            bool run = active;
+            tv.flags = flags0;
+            for (;;) {
+                if (run) st = hive::insert_deferred_one<P>(tv, hive::key_of(e), hive::val_of(e));
+                if (!d.sq) break;
+                const bool hand_on = run && st == hive::kStDefer;
+                const unsigned m = __ballot_sync(0xffffffffu, hand_on);
+                if (!m) break;
+                const int leader = __ffs(m) - 1;
+                u64 base = 0;
+                if ((int)lane == leader) base = atomicAdd(d.sn, (u64)__popc(m));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                const u64 pos = base + __popc(m & ((1u << lane) - 1u));
+                if (hand_on && pos < d.scap) {
+                    d.sq[pos] = __ldcs(d.q + q);
+                    d.skv[pos] = e;
+                }
+                run = hand_on && pos >= d.scap;
+                if (!__any_sync(0xffffffffu, run)) break;
+                tv.flags = (flags0 & ~hive::kFlagDeferStash) | hive::kFlagResumed;
+            }
+            // a handed-on op's status is written by the third pass
+            if (status && active && st != hive::kStInserted && st != hive::kStDefer) status[__ldcs(d.q + q)] = st;
         }
     } else {
-        for (; j < cnt; j += stride) {
+        for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += stride) {
             const uint32_t i = d.q[defer_slot(j, cnt, d.permute)];
             const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals[i]);
             if (status) status[i] = st;
@@ -237,11 +277,25 @@ __global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, co
     }
 }
 
+// The second pass and, for ops it handed on, the third.
 template <int P>
 void launch_second_pass(unsigned grid, cudaStream_t s, const hive::Table& t, const uint32_t* keys,
                         const uint32_t* vals, uint8_t* status, const Defer& d) {
-    if (d.kv) k_insert_deferred<P, true><<<grid, kBlock, 0, s>>>(t, keys, vals, status, d);
-    else k_insert_deferred<P, false><<<grid, kBlock, 0, s>>>(t, keys, vals, status, d);
+    if (!d.kv) {
+        k_insert_deferred<P, false><<<grid, kBlock, 0, s>>>(t, keys, vals, status, d);
+        return;
+    }
+    hive::Table t2 = t;
+    if (d.sq) t2.flags |= hive::kFlagDeferStash;
+    k_insert_deferred<P, true><<<grid, kBlock, 0, s>>>(t2, keys, vals, status, d);
+    if (!d.sq) return;
+    Defer d3{d.sq, d.sn};
+    d3.kv = d.skv;
+    d3.cap = d.scap;
+    hive::Table t3 = t;
+    t3.flags |= hive::kFlagResumed;
+    const unsigned g3 = (unsigned)std::min<uint64_t>(grid, (d.scap + kBlock - 1) / kBlock);
+    k_insert_deferred<P, true><<<g3, kBlock, 0, s>>>(t3, keys, vals, status, d3);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -885,21 +939,46 @@ int table_view(hive_table* h, cudaStream_t s, hive::Table* tv) {
 // The deferred-op queue for a batch of n ops; grows (synchronously) to the largest batch seen.
 // Batches of 2^32 ops or more run without deferral.
 // The queue of a batch of n ops: n indices and, for bulk inserts (with_kv), n packed kv words.
+// Capacity of the third-pass queue for a batch of n ops: ops reach it only after a first pass
+// found both buckets full and an eviction found no victim (about 0.25 % of the ops of a bulk
+// insert at load factor 0.9); further ones are finished in the second pass.
+uint64_t stash_queue_cap(uint64_t n) { return n / 16 + 1024; }
+
+// The queue of a batch of n ops: n indices and, for bulk inserts (with_kv), n packed kv words
+// and the third-pass queue (stash_queue_cap(n) indices and kv words).
 int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d, bool with_kv = false) {
     *d = Defer{nullptr, h->scratch + 1};
     if (n > 0xFFFFFFFFull) return HIVE_OK;
+    const auto layout = [](uint64_t cap, size_t* kv, size_t* sq, size_t* skv, size_t* total) {
+        const uint64_t sc = stash_queue_cap(cap);
+        *kv = align256((size_t)cap * 4);
+        *sq = align256(*kv + (size_t)cap * 8);
+        *skv = align256(*sq + (size_t)sc * 4);
+        *total = *skv + (size_t)sc * 8;
+    };
+    size_t okv, osq, oskv, total;
     if (n > h->defer_cap) {
         HIVE_CUDA(cudaDeviceSynchronize());
         if (h->defer_q) cudaFree(h->defer_q);
         h->defer_q = nullptr;
         h->defer_cap = 0;
-        cudaError_t e = cudaMalloc(&h->defer_q, align256((size_t)n * 4) + (size_t)n * 8);
+        layout(n, &okv, &osq, &oskv, &total);
+        cudaError_t e = cudaMalloc(&h->defer_q, total);
         if (e != cudaSuccess) return cuda_fail(e);
         h->defer_cap = n;
     }
     HIVE_CUDA(cudaMemsetAsync(h->scratch + 1, 0, 8, s));
     d->q = h->defer_q;
-    if (with_kv) d->kv = (u64*)((char*)h->defer_q + align256((size_t)h->defer_cap * 4));
+    if (with_kv) {
+        layout(h->defer_cap, &okv, &osq, &oskv, &total);
+        char* base = (char*)h->defer_q;
+        d->kv = (u64*)(base + okv);
+        d->sq = (uint32_t*)(base + osq);
+        d->skv = (u64*)(base + oskv);
+        d->sn = h->scratch + 6;
+        d->scap = stash_queue_cap(h->defer_cap);
+        HIVE_CUDA(cudaMemsetAsync(d->sn, 0, 8, s));
+    }
     return HIVE_OK;
 }
 
