@@ -83,10 +83,11 @@ constexpr uint32_t kFlagPrimaryFirst = 8u;  // set on the launch's copy only: it
 constexpr uint32_t kFlagUntagged = 2u;  // set on the launch's copy only: the launch neither reads
                                         // nor keeps the tag words (a bulk insert that rebuilds them
                                         // after it, or a table too large for them to stay in L2)
-constexpr uint32_t kFlagDeferStash = 16u;  // set on the launch's copy only: a locked-path insert
-                                           // whose eviction found no victim returns kStDefer
-                                           // (lock released) instead of using the stash, for a
-                                           // later pass that finishes such ops together
+constexpr uint32_t kFlagHandOn = 16u;  // set on the launch's copy only: a locked-path insert
+                                      // whose H0 lock is taken at its first attempt, or whose
+                                      // eviction found no victim, returns kStDefer (holding no
+                                      // lock) instead of waiting or using the stash, for a later
+                                      // pass that finishes such ops together
 constexpr uint32_t kFlagResumed = 32u;     // set on the launch's copy only: the ops were counted
                                            // on the slow path by the pass that handed them on
 
@@ -848,7 +849,7 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         // Handed on (the caller releases the lock): ops bound for the stash take several more
         // dependent steps than an eviction, so finishing them in a later pass of their own keeps
         // them from holding up the warps of the eviction pass.
-        if (t.flags & kFlagDeferStash) return kStDefer;
+        if (t.flags & kFlagHandOn) return kStDefer;
         // Stage D: the canonical bucket's stash.  Its flag is raised before the entry is
         // written, so a reader that finds the entry also finds the flag set.
         if (!(atomicOr(t.stash_bits + (b0 >> 5), 1u << (b0 & 31)) & (1u << (b0 & 31)))) fence_acq_rel();
@@ -1129,7 +1130,15 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
 template <int P>
 __device__ __noinline__ uint8_t insert_locked_path(const Table& t, uint32_t k, u64 kv, uint32_t b0, uint32_t b1) {
     if (!(t.flags & kFlagResumed)) count(t, kCtrSlowPath);
-    if (!lock_bucket(t, b0)) return kStError;
+    if (t.flags & kFlagHandOn) {
+        // one attempt: an op that would wait for the lock is handed on instead of stalling its warp
+        if (!lock_byte_try(t, b0)) {
+            count(t, kCtrLockWaits);
+            return kStDefer;
+        }
+    } else if (!lock_bucket(t, b0)) {
+        return kStError;
+    }
     uint8_t st = insert_locked<P>(t, k, kv, b0, b1);
     unlock_bucket(t, b0);
     return st;

@@ -158,8 +158,8 @@ struct Defer {
     // outcome, leaves the byte alone: a scattered 1-byte write costs a DRAM read and write).
     u64* kv = nullptr;
     u64 cap = ~0ull;  // entries the queue holds (a later count may pass it: see k_insert_deferred)
-    // Bulk inserts: where the second pass hands on the ops whose eviction found no victim (their
-    // index, packed kv and count), for a third pass that takes them to the stash.
+    // Bulk inserts: where the second pass hands on the ops it does not finish (their index, packed
+    // kv and count): those whose H0 lock was taken and those whose eviction found no victim.
     uint32_t* sq = nullptr;
     u64* skv = nullptr;
     u64* sn = nullptr;
@@ -219,9 +219,10 @@ __global__ void __launch_bounds__(kBlock, (kDefer && hive::mode_base(kMode) == h
 
 // Second pass: the deferred inserts, grid-stride over the queue.  kKV: the queue carries the ops'
 // packed kv (Defer::kv) and the statuses are provisionally kStInserted; else the ops are gathered
-// from the batch by index and every status is written.  With Defer::sq (and kFlagDeferStash on
-// the view) an op whose eviction found no victim is handed on to that queue for a third pass
-// (this kernel again, over the handed-on ops); one that finds it full is finished here.
+// from the batch by index and every status is written.  With Defer::sq (and kFlagHandOn on
+// the view) an op whose H0 lock was taken or whose eviction found no victim is handed on to that
+// queue for a third pass (this kernel again, over the handed-on ops); one that finds the queue
+// full is finished here.
 template <int P, bool kKV>
 __global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, const uint32_t* __restrict__ keys,
                                                             const uint32_t* __restrict__ vals,
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, co
                 }
                 run = hand_on && pos >= d.scap;
                 if (!__any_sync(0xffffffffu, run)) break;
-                tv.flags = (flags0 & ~hive::kFlagDeferStash) | hive::kFlagResumed;
+                tv.flags = (flags0 & ~hive::kFlagHandOn) | hive::kFlagResumed;
             }
             // a handed-on op's status is written by the third pass
             if (status && active && st != hive::kStInserted && st != hive::kStDefer) status[__ldcs(d.q + q)] = st;
@@ -286,7 +287,7 @@ void launch_second_pass(unsigned grid, cudaStream_t s, const hive::Table& t, con
         return;
     }
     hive::Table t2 = t;
-    if (d.sq) t2.flags |= hive::kFlagDeferStash;
+    if (d.sq) t2.flags |= hive::kFlagHandOn;
     k_insert_deferred<P, true><<<grid, kBlock, 0, s>>>(t2, keys, vals, status, d);
     if (!d.sq) return;
     Defer d3{d.sq, d.sn};
@@ -940,8 +941,8 @@ int table_view(hive_table* h, cudaStream_t s, hive::Table* tv) {
 // Batches of 2^32 ops or more run without deferral.
 // The queue of a batch of n ops: n indices and, for bulk inserts (with_kv), n packed kv words.
 // Capacity of the third-pass queue for a batch of n ops: ops reach it only after a first pass
-// found both buckets full and an eviction found no victim (about 0.25 % of the ops of a bulk
-// insert at load factor 0.9); further ones are finished in the second pass.
+// found both buckets full and then found H0's lock taken or no eviction victim (about 0.5 % of
+// the ops of a bulk insert at load factor 0.9); further ones are finished in the second pass.
 uint64_t stash_queue_cap(uint64_t n) { return n / 16 + 1024; }
 
 // The queue of a batch of n ops: n indices and, for bulk inserts (with_kv), n packed kv words
