@@ -122,13 +122,15 @@ int hive_clear(hive_table* t, void* stream);
 /* Bulk upsert of n (key, value) pairs; status[i] = HIVE_ST_*.  status may be NULL.
  * Replaces hive_insert_kernel launched by run_hash_table_benchmark
  * (include/hive_kernels.cuh:205-266, src/hive_dispatch.cu:134-148), with explicit values
- * instead of the reference's value = key + 1 (include/hive_kernels.cuh:238). */
+ * instead of the reference's value = key + 1 (include/hive_kernels.cuh:238).  The table keeps a
+ * queue for the ops that need a second pass, about 12.75 bytes per op of the largest batch, grown
+ * with cudaMalloc (stream-synchronising) the first time a batch is larger than any before. */
 int hive_insert(hive_table* t, const uint32_t* keys, const uint32_t* values, uint64_t n,
                 uint8_t* status, void* stream);
 
 /* hive_insert without any device allocation.  No counterpart in the reference.
  *
- * hive_insert keeps its second-pass queue (4 bytes per op) in device memory that it allocates,
+ * hive_insert keeps its second-pass queue (about 13 bytes per op) in device memory that it allocates,
  * and grows with cudaMalloc the first time a batch is larger than any before.  Some callers
  * cannot allow that: a service that hands all device memory to its own pool up front, a
  * latency-bound loop where cudaMalloc/cudaFree would stall the device, code under an allocator
