@@ -477,25 +477,19 @@ __global__ void __launch_bounds__(kBlock) k_apply(hive::Table t, const uint8_t* 
     uint8_t st = 0;
     if (active)
         st = apply_one<P, kDefer, kMode>(t, __ldcs(types + i), __ldcs(keys + i), vals ? __ldcs(vals + i) : 0u, &o);
-    if (kDefer) defer_push(d, st == hive::kStDefer, i);
-    if (!active || st == hive::kStDefer) return;
+    // Only inserts defer.  Their queue entries carry key and value (Defer::kv), and the later
+    // insert passes (k_insert_deferred) write only statuses that differ from the provisional
+    // kStInserted; a deferred insert's out value is 0.
+    u64 kv = 0;
+    if (kDefer && st == hive::kStDefer && d.kv) kv = hive::pack(__ldcg(keys + i), vals ? __ldcg(vals + i) : 0u);
+    if (kDefer) defer_push(d, st == hive::kStDefer, i, kv);
+    if (!active) return;
+    if (st == hive::kStDefer) {
+        if (!d.kv) return;
+        st = hive::kStInserted;
+    }
     if (status) __stcs(status + i, st);
     if (outv) __stcs(outv + i, o);
-}
-
-// Second pass of k_apply: the deferred inserts (their out value is 0).
-template <int P>
-__global__ void __launch_bounds__(kBlock, 4) k_apply_deferred(hive::Table t, const uint32_t* __restrict__ keys,
-                                                           const uint32_t* __restrict__ vals,
-                                                           uint8_t* __restrict__ status, uint32_t* __restrict__ outv,
-                                                           Defer d) {
-    const u64 cnt = *d.n;
-    for (u64 j = (u64)blockIdx.x * kBlock + threadIdx.x; j < cnt; j += (u64)gridDim.x * kBlock) {
-        const uint32_t i = d.q[defer_slot(j, cnt, d.permute)];
-        const uint8_t st = hive::insert_deferred_one<P>(t, keys[i], vals ? vals[i] : 0u);
-        if (status) status[i] = st;
-        if (outv) outv[i] = 0u;
-    }
 }
 
 // A sequence of mixed batches in one cooperative launch.  Per batch: a first pass over its ops
@@ -945,8 +939,13 @@ int table_view(hive_table* h, cudaStream_t s, hive::Table* tv) {
 // the ops of a bulk insert at load factor 0.9); further ones are finished in the second pass.
 uint64_t stash_queue_cap(uint64_t n) { return n / 16 + 1024; }
 
+// Batches from this size on hand ops on to a third pass (Defer::sq).  The extra launch costs a
+// few microseconds, which a stream of small mixed batches (2^10..2^20 ops) pays thousands of
+// times: measured there, it lowered the plain batched workload from 3.0 to 2.6 G ops/s.
+constexpr uint64_t kHandOnMinOps = 1ull << 21;
+
 // The queue of a batch of n ops: n indices and, for bulk inserts (with_kv), n packed kv words
-// and the third-pass queue (stash_queue_cap(n) indices and kv words).
+// and the third-pass queue (stash_queue_cap(n) indices and kv words), used for n >= kHandOnMinOps.
 int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d, bool with_kv = false) {
     *d = Defer{nullptr, h->scratch + 1};
     if (n > 0xFFFFFFFFull) return HIVE_OK;
@@ -974,11 +973,13 @@ int prepare_defer(hive_table* h, uint64_t n, cudaStream_t s, Defer* d, bool with
         layout(h->defer_cap, &okv, &osq, &oskv, &total);
         char* base = (char*)h->defer_q;
         d->kv = (u64*)(base + okv);
-        d->sq = (uint32_t*)(base + osq);
-        d->skv = (u64*)(base + oskv);
-        d->sn = h->scratch + 6;
-        d->scap = stash_queue_cap(h->defer_cap);
-        HIVE_CUDA(cudaMemsetAsync(d->sn, 0, 8, s));
+        if (n >= kHandOnMinOps) {
+            d->sq = (uint32_t*)(base + osq);
+            d->skv = (u64*)(base + oskv);
+            d->sn = h->scratch + 6;
+            d->scap = stash_queue_cap(h->defer_cap);
+            HIVE_CUDA(cudaMemsetAsync(d->sn, 0, 8, s));
+        }
     }
     return HIVE_OK;
 }
@@ -1636,7 +1637,7 @@ int hive_apply_ops(hive_table* h, const uint8_t* types, const uint32_t* keys, co
     cudaStream_t s = (cudaStream_t)stream;
     if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
     Defer d;
-    int rc = prepare_defer(h, n, s, &d);
+    int rc = prepare_defer(h, n, s, &d, true);
     if (rc) return rc;
     hive::Table tv;
     if (int vrc = table_view(h, s, &tv)) return vrc;
@@ -1645,8 +1646,8 @@ int hive_apply_ops(hive_table* h, const uint8_t* types, const uint32_t* keys, co
                          out_values, d);
     else
         HIVE_DISPATCH_D(k_apply, d, grid_for(n), kBlock, s, tv, types, keys, values, n, status, out_values, d);
-    if (d.q)
-        HIVE_DISPATCH(k_apply_deferred, second_pass_grid(h, n), kBlock, s, tv, keys, values, status, out_values, d);
+    // the deferred inserts: the bulk insert's second pass and the third pass over what it hands on
+    if (d.q) HIVE_DISPATCH_FN(launch_second_pass, second_pass_grid(h, n), s, tv, keys, values, status, d);
     return launch_check();
 }
 
