@@ -207,7 +207,25 @@ __global__ void __launch_bounds__(kBlock, (kDefer && hive::mode_base(kMode) == h
     const uint64_t i = lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < hi;
     uint8_t st = hive::kStFail;
-    if (active) st = hive::insert_one<P, kDefer, kMode>(t, __ldcs(keys + i), __ldcs(vals + i));
+    if constexpr (kDefer && hive::mode_base(kMode) == hive::kModeMono && (kMode & hive::kModeUntagged) &&
+                  !(kMode & hive::kModePrimary)) {
+        // Bulk first pass: each bucket read is one request shared by a lane pair (every lane of
+        // the warp takes part in both rounds, so nothing here returns early).
+        const uint32_t k = active ? __ldcs(keys + i) : 0u;
+        const uint32_t v = active ? __ldcs(vals + i) : 0u;
+        const bool live = k != 0u;
+        const u64 kv = hive::pack(k, v);
+        const uint32_t b0 = live ? hive::bucket_addr(t, hive::Policy<P>::h0(k)) : 0u;
+        const uint32_t b1 = live ? hive::bucket_addr(t, hive::Policy<P>::h1(k)) : 0u;
+        const uint32_t m0 = hive::warp_bucket_masks(t.slots, live, b0, k);
+        if (live) st = hive::claim_from_masks(t, b0, k, kv, m0);
+        const bool need1 = live && !st && b1 != b0;
+        const uint32_t m1 = hive::warp_bucket_masks(t.slots, need1, b1, k);
+        if (need1) st = hive::claim_from_masks(t, b1, k, kv, m1);
+        if (live && !st) st = hive::kStDefer;
+    } else if (active) {
+        st = hive::insert_one<P, kDefer, kMode>(t, __ldcs(keys + i), __ldcs(vals + i));
+    }
     // a deferred op's key and value are read again (L2 hits: the lines were just streamed in)
     // rather than kept live across the insert
     u64 kv = 0;
