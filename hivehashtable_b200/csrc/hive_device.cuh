@@ -68,7 +68,7 @@ enum {
     kCtrFailed = 3,       // inserts that could not be placed
     kCtrLockTimeout = 4,  // lock waits that expired
     kCtrRetryOut = 5,     // CAS retry budgets that ran out
-    kCtrDupFixed = 6,     // duplicate copies removed after racing same-key inserts
+    kCtrDupFixed = 6,     // unused: claims of one key are serialised, so no copy is ever removed
     kCtrLockWaits = 7,    // lock attempts that found the bucket locked (contention)
     kCtrError = 15,       // sticky error bits (kErr*)
 };
@@ -664,35 +664,6 @@ __device__ __forceinline__ int increment_in(u64* p, uint32_t k, uint32_t* nv) {
     return 1;
 }
 
-// After claiming slot j of bucket p for k while deletes may run (kFlagHoles), two inserts of the
-// same key can claim different slots.  Keep the lower-indexed copy; whichever of the two racing
-// inserts sees the other removes the higher one (a CAS from the exact value, so at most one
-// removal happens and nothing else is ever removed).  Returns true if this op's own copy was
-// the one removed.  b is the bucket's index (the removed copy's fingerprint is cleared).
-__device__ __forceinline__ bool resolve_duplicate(const Table& t, uint32_t b, uint32_t k, int j, u64 kv) {
-    u64* p = t.slots + (size_t)b * kSlots;
-    __threadfence();
-    Bucket B;
-    load_bucket(p, B);
-    uint32_t m = match_mask(B, k) & ~(1u << j);
-    if (!m) return false;
-    int o = __ffs(m) - 1;
-    if (o < j) {
-        if (cas64(p + j, kv, 0ull) == kv) {
-            tag_clear(t, b, j);
-            count(t, kCtrDupFixed);
-            return true;
-        }
-        return false;
-    }
-    u64 theirs = slot_at(B, o);
-    if (cas64(p + o, theirs, 0ull) == theirs) {
-        tag_clear(t, b, o);
-        count(t, kCtrDupFixed);
-    }
-    return false;
-}
-
 // ---------------------------------------------------------------------------------------------
 // Insert = upsert (S2).  Four stages as in include/hive_hash_insert.cuh:898-1042:
 //   A  try-replace in the candidate buckets and the canonical stash,
@@ -837,7 +808,6 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
     u64* B0p = t.slots + (size_t)b0 * kSlots;
     u64* B1p = t.slots + (size_t)b1 * kSlots;
     u64* Sp = t.stash + (size_t)b0 * kSlots;
-    const bool holes = t.flags & kFlagHoles;
     for (int r = 0; r < kRetryLimit; ++r) {
         Bucket B0, B1;
         load_bucket(B0p, B0);
@@ -867,7 +837,6 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
             if (cas64(B0p + j, 0ull, kv) == 0ull) {
                 tag_set(t, b0, j, tag_of(k));
                 if (__popc(e) == 1) mark_full(t, b0);
-                if (holes && resolve_duplicate(t, b0, k, j, kv)) return kStUpdated;
                 return kStInserted;
             }
             continue;
@@ -878,7 +847,6 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
             if (cas64(B1p + j, 0ull, kv) == 0ull) {
                 tag_set(t, b1, j, tag_of(k));
                 if (__popc(e) == 1) mark_full(t, b1);
-                if (holes && resolve_duplicate(t, b1, k, j, kv)) return kStUpdated;
                 return kStInserted;
             }
             continue;
@@ -1160,7 +1128,13 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
         return claim_or_update<kTagged>(t, b1, k, kv);
     }
     if (kTagged && (kMode & kModeUnique) && tagged(t)) return insert_holes_unique<kPrimaryOnly>(t, k, kv, b0, b1);
-    // With holes a key may sit in H1 or the stash while H0 has room: scan all three first.
+    // With holes a key may sit in H1 or the stash while H0 has room: look in all three and update
+    // a copy in place.  A new key is claimed only on the locked path, under H0's lock: two inserts
+    // of one key that both find it absent are serialised there, and the second one's rescan under
+    // the lock finds the first one's copy, so no key ever gets two copies.  (A claim made without
+    // the lock could land in H0 while a racing insert of the same key, which found H0 full before
+    // a delete freed a slot, lands in H1 or the stash.  The reference guards the same race with a
+    // duplicate check under the canonical bucket's lock, include/hive_hash_insert.cuh:522-541.)
     u64* Sp = t.stash + (size_t)b0 * kSlots;
     for (int r = 0; r < kRetryLimit; ++r) {
         Bucket B0, B1;
@@ -1185,22 +1159,7 @@ __device__ __forceinline__ uint8_t insert_lockfree(const Table& t, uint32_t k, u
             if (u == 1) return kStUpdated;
             if (u < 0) continue;
         }
-        uint32_t e = empty_mask(B0);
-        u64* Cp = B0p;
-        uint32_t cb = b0;
-        if (!e && b1 != b0 && !kPrimaryOnly) {
-            e = empty_mask(B1);
-            Cp = B1p;
-            cb = b1;
-        }
-        if (!e) return 0;
-        int j = __ffs(e) - 1;
-        if (cas64(Cp + j, 0ull, kv) == 0ull) {
-            if (kTagged) tag_set(t, cb, j, tag_of(k));
-            if (__popc(e) == 1) mark_full(t, cb);
-            if (kMode & kModeUnique) return kStInserted;
-            return resolve_duplicate(t, cb, k, j, kv) ? kStUpdated : kStInserted;
-        }
+        return 0;
     }
     return 0;
 }

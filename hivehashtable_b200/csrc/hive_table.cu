@@ -712,10 +712,19 @@ __global__ void __launch_bounds__(kBlock) k_count_unplaced(const uint8_t* __rest
     if ((threadIdx.x & 31) == 0 && m) atomicAdd(cnt, (u64)__popc(m));
 }
 
+// Copies of k in bucket (or stash bucket) p.
+__device__ __forceinline__ u64 copies_in(const u64* p, uint32_t k) {
+    hive::Bucket B;
+    hive::load_bucket_ro(p, B);
+    return (u64)__popc(hive::match_mask(B, k));
+}
+
 // Structural check of buckets [0, nb) and their stashes; out[HIVE_VERIFY_*] counts violations:
 // a slot whose tag byte is not its key's fingerprint, a key in neither of its buckets (a stash
-// entry not under its canonical bucket), a key twice in one bucket, and -- only when the table has
-// no holes (strict) -- a free slot with a nonzero tag byte.
+// entry not under its canonical bucket), a key with more than one copy (twice in one bucket, or
+// in more than one of its H0, its H1 and H0's stash: each extra copy counted once, by the copy
+// in the earlier of those places), and -- only when the table has no holes (strict) -- a free
+// slot with a nonzero tag byte.
 template <int P>
 __global__ void k_verify(hive::Table t, uint64_t nb, bool strict, u64* out) {
     const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -734,15 +743,22 @@ __global__ void k_verify(hive::Table t, uint64_t nb, bool strict, u64* out) {
         }
         const uint32_t k = hive::key_of(kv);
         bad[HIVE_VERIFY_TAG_MISMATCH] += tags && byte != hive::tag_of(k);
-        bad[HIVE_VERIFY_MISPLACED] +=
-            hive::bucket_addr(t, hive::Policy<P>::h0(k)) != b && hive::bucket_addr(t, hive::Policy<P>::h1(k)) != b;
+        const uint32_t c0 = hive::bucket_addr(t, hive::Policy<P>::h0(k));
+        const uint32_t c1 = hive::bucket_addr(t, hive::Policy<P>::h1(k));
+        bad[HIVE_VERIFY_MISPLACED] += c0 != b && c1 != b;
         for (int q = 0; q < j; ++q) bad[HIVE_VERIFY_DUPLICATE] += hive::key_of(B.s[q]) == k;
+        if (c0 == b && c1 != b) bad[HIVE_VERIFY_DUPLICATE] += copies_in(t.slots + (size_t)c1 * hive::kSlots, k);
+        if ((c0 == b || c1 == b) && ((t.stash_bits[c0 >> 5] >> (c0 & 31)) & 1u))
+            bad[HIVE_VERIFY_DUPLICATE] += copies_in(t.stash + (size_t)c0 * hive::kSlots, k);
     }
     if ((t.stash_bits[b >> 5] >> (b & 31)) & 1u) {
         hive::load_bucket_ro(t.stash + b * hive::kSlots, B);
         for (int j = 0; j < hive::kSlots; ++j)
-            if (B.s[j])
-                bad[HIVE_VERIFY_MISPLACED] += hive::bucket_addr(t, hive::Policy<P>::h0(hive::key_of(B.s[j]))) != b;
+            if (B.s[j]) {
+                const uint32_t k = hive::key_of(B.s[j]);
+                bad[HIVE_VERIFY_MISPLACED] += hive::bucket_addr(t, hive::Policy<P>::h0(k)) != b;
+                for (int q = 0; q < j; ++q) bad[HIVE_VERIFY_DUPLICATE] += hive::key_of(B.s[q]) == k;
+            }
     }
     for (int c = 0; c < HIVE_VERIFY_COUNT; ++c)
         if (bad[c]) atomicAdd(out + c, bad[c]);

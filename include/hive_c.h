@@ -65,9 +65,11 @@ extern "C" {
 #define HIVE_HINT_UNIQUE_KEYS 4u  /* caller guarantees each key appears at most once in the batch
                                      (as a coalescing server or a deduplicated batch does): on a
                                      table that has had deletes, inserts then find an existing
-                                     copy and a free slot from the per-slot fingerprints and skip
-                                     the check for a racing second insert of their key.  A batch
-                                     that breaks the promise may keep two copies of a key    */
+                                     copy and a free slot from the per-slot fingerprints and
+                                     claim without the canonical bucket's lock (without the hint
+                                     a new key is claimed only under that lock, which serialises
+                                     the inserts of one key).  A batch that breaks the promise
+                                     may keep two copies of a key                            */
 
 /* ---- counters (hive_counters) ---------------------------------------------------------------- */
 #define HIVE_CTR_SLOW_PATH 0    /* inserts whose canonical bucket was full                     */
@@ -76,7 +78,7 @@ extern "C" {
 #define HIVE_CTR_FAILED 3       /* inserts that could not be placed                            */
 #define HIVE_CTR_LOCK_TIMEOUT 4 /* bucket-lock waits that expired                              */
 #define HIVE_CTR_RETRY_OUT 5    /* CAS retry budgets that ran out                              */
-#define HIVE_CTR_DUP_FIXED 6    /* duplicate copies removed after racing same-key inserts      */
+#define HIVE_CTR_DUP_FIXED 6    /* always 0: inserts of one key claim under one lock, no copies */
 #define HIVE_CTR_LOCK_WAITS 7   /* bucket-lock attempts that found the lock taken (contention) */
 #define HIVE_CTR_ERROR 15       /* sticky error bits                                           */
 #define HIVE_NUM_COUNTERS 16
@@ -255,7 +257,8 @@ int hive_check(hive_table* t, void* stream);
 
 /* Structural check of the table on the device (synchronises `stream`): out[HIVE_VERIFY_*] counts
  * slots whose per-slot fingerprint byte is not their key's, keys outside both of their buckets
- * (stash entries outside their canonical bucket's stash), keys held twice in one bucket, and --
+ * (stash entries outside their canonical bucket's stash), extra copies of a key (twice in one
+ * bucket, or in more than one of its two buckets and its canonical stash), and --
  * on a table with no delete or resize since the last clear -- free slots with a nonzero
  * fingerprint.  All zero on a sound table.  Replaces the reference's post-run table checks
  * (count_occupancy_kernel, src/hive_dispatch.cu:169-176; freeMask copy-back,

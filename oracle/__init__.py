@@ -46,6 +46,9 @@ def lib() -> ctypes.CDLL:
             "hive_oracle_map_erase": (None, [_P, _P, _U64, _P]),
             "hive_oracle_map_apply": (None, [_P, _P, _P, _P, _U64, _P, _P, _P]),
             "hive_oracle_map_dump": (_U64, [_P, _P, _P, _U64]),
+            "hive_oracle_serial_selftest": (_U64, [_U64, _U64, _I32]),
+            "hive_oracle_map_check_serial": (_U64, [_P, _P, _P, _P, _P, _U64, _P, _P, _P, _P, _U64,
+                                                    ctypes.POINTER(_U64)]),
             "hive_oracle_cpu_new": (_P, [_I32, _U64, _I32]),
             "hive_oracle_cpu_free": (None, [_P]),
             "hive_oracle_cpu_failed": (_U64, [_P]),
@@ -157,12 +160,36 @@ class ReplayMap:
         lib().hive_oracle_map_apply(self._h, _p(t), _p(k), _p(v), k.size, _p(m), _p(st), _p(ov))
         return st, ov
 
+    def check_serial(self, types, keys, vals, launch, status, out_vals, fin_keys, fin_vals):
+        """Per-key serialisation check of concurrent launches (hive_oracle_map_check_serial): for
+        every key, some order of its ops that keeps launch order (any order inside a launch) must
+        give each observed status / out value and the key's state in the final contents
+        (fin_keys sorted).  Returns (number of keys with no such order, lowest op index of one of
+        them or -1); with 0 the map advances to the final state of every key the run touched."""
+        t = np.ascontiguousarray(types, dtype=np.uint8)
+        k, v = _u32(keys), _u32(vals)
+        b = _u32(launch)
+        st = np.ascontiguousarray(status, dtype=np.uint8)
+        ov = _u32(out_vals)
+        fk, fv = _u32(fin_keys), _u32(fin_vals)
+        assert t.size == k.size == v.size == b.size == st.size == ov.size and fk.size == fv.size
+        first = ctypes.c_uint64()
+        bad = lib().hive_oracle_map_check_serial(self._h, _p(t), _p(k), _p(v), _p(b), k.size, _p(st), _p(ov),
+                                                 _p(fk), _p(fv), fk.size, ctypes.byref(first))
+        return int(bad), (-1 if bad == 0 else int(first.value))
+
     def dump(self):
         n = len(self)
         k = np.empty(n, dtype=np.uint32)
         v = np.empty(n, dtype=np.uint32)
         lib().hive_oracle_map_dump(self._h, _p(k), _p(v), n)
         return k, v
+
+
+def serial_selftest(seed: int, trials: int, max_ops: int) -> int:
+    """Disagreements between the closed-form and the searched per-key serialisation checks on
+    random single-launch groups (0 expected)."""
+    return int(lib().hive_oracle_serial_selftest(seed, trials, max_ops))
 
 
 # ---- multithreaded CPU bucketed cuckoo table ----------------------------------------------------

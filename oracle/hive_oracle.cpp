@@ -11,6 +11,8 @@
 //   3. A std::unordered_map replay: the semantic oracle for every op result and for the final
 //      key->value set (reference semantics S1-S6 of include/hive_hash_insert.cuh,
 //      include/hive_hash_lookup.cuh, include/hive_hash_delete.cuh).
+//   3b. The per-key serialisation check of concurrent launches: every op result and final state
+//      must come from some order of each key's ops that keeps launch order.
 //   4. A multithreaded CPU bucketed cuckoo table (8-slot buckets, two hashes, CAS slot claims,
 //      depth-1 eviction under bucket locks, per-bucket overflow stash) driven by std::thread:
 //      the reported CPU baseline for the same policy.
@@ -324,6 +326,185 @@ struct ReplayMap {
     std::unordered_map<uint32_t, uint32_t> m;
 };
 
+// ---------------------------------------------------------------------------------------------
+// 3b. Concurrent batches: the per-key serialisation check
+// ---------------------------------------------------------------------------------------------
+// The ops of one launch are unordered (the reference's mixed kernel runs one op per thread with
+// no order among them, include/hive_kernels.cuh:119-192); launches are ordered by the stream.
+// A run is correct when, for every key, some order of that key's ops that keeps launch order
+// (any order inside a launch) reproduces every observed result of those ops and the key's final
+// state.  Ops on different keys commute, so keys are checked one at a time.
+
+struct SerialOp {
+    uint8_t type;   // 0 insert, 1 lookup, 2 delete, 3 increment, other: no-op
+    uint32_t val;   // insert value
+    uint8_t st;     // observed status
+    uint32_t ov;    // observed out value
+};
+
+// Applies op o to the key's state (present, value) as the replay does; false when the observed
+// result cannot come from that state.  Insert statuses: 1 or 3 new key, 2 updated, 0 not placed
+// (possible only while the key is absent; no effect).
+inline bool serial_step(const SerialOp& o, bool& present, uint32_t& value) {
+    switch (o.type) {
+        case 0:
+            if (o.ov != 0) return false;
+            if (o.st == 0) return !present;
+            if (present) {
+                if (o.st != 2) return false;
+            } else if (o.st != 1 && o.st != 3) {
+                return false;
+            }
+            present = true;
+            value = o.val;
+            return true;
+        case 1:
+            return present ? (o.st == 1 && o.ov == value) : (o.st == 0 && o.ov == 0);
+        case 2:
+            if (o.ov != 0 || o.st != (present ? 1 : 0)) return false;
+            present = false;
+            return true;
+        case 3:
+            if (!present) return o.st == 0 && o.ov == 0;
+            if (o.st != 1 || o.ov != value + 1u) return false;
+            value += 1u;
+            return true;
+        default:
+            return o.st == 0 && o.ov == 0;
+    }
+}
+
+struct SerialState {
+    uint64_t used, rest;  // rest = launch << 33 | present << 32 | value
+    bool operator==(const SerialState& o) const { return used == o.used && rest == o.rest; }
+};
+struct SerialStateHash {
+    size_t operator()(const SerialState& s) const { return (size_t)(s.used * 0x9E3779B97F4A7C15ull ^ s.rest); }
+};
+
+struct SerialSearch {
+    const std::vector<std::vector<SerialOp>>* groups;  // the key's ops per launch, launches in order
+    bool fin_present;
+    uint32_t fin_value;
+    int64_t budget;  // search steps left
+    std::unordered_set<SerialState, SerialStateHash> dead;  // states known to lead nowhere
+
+    // Ops of launch g not in `used` in some order, then the later launches.  Among identical
+    // unused ops only the first is tried (they lead to the same states); a state already shown
+    // to fail is not searched again.
+    bool run(size_t g, uint64_t used, bool present, uint32_t value) {
+        const auto& gs = *groups;
+        if (g == gs.size()) return present == fin_present && (!present || value == fin_value);
+        const auto& G = gs[g];
+        if (used == (G.size() == 64 ? ~0ull : (1ull << G.size()) - 1ull)) return run(g + 1, 0, present, value);
+        const SerialState key{used, ((uint64_t)g << 33) | ((uint64_t)present << 32) | value};
+        if (dead.count(key)) return false;
+        if (search(g, used, present, value)) return true;
+        dead.insert(key);
+        return false;
+    }
+
+    bool search(size_t g, uint64_t used, bool present, uint32_t value) {
+        const auto& G = (*groups)[g];
+        for (size_t j = 0; j < G.size(); ++j) {
+            if ((used >> j) & 1ull) continue;
+            bool twin = false;
+            for (size_t q = 0; q < j && !twin; ++q)
+                twin = !((used >> q) & 1ull) && G[q].type == G[j].type && G[q].val == G[j].val &&
+                       G[q].st == G[j].st && G[q].ov == G[j].ov;
+            if (twin) continue;
+            bool p = present;
+            uint32_t v = value;
+            if (!serial_step(G[j], p, v)) continue;
+            if (--budget < 0) return false;
+            if (run(g, used | (1ull << j), p, v)) return true;
+        }
+        return false;
+    }
+};
+
+// One launch's ops on a key, none of them an increment, from a known state: decided without a
+// search.  Without increments the state after a write depends on that write alone: a new-key
+// insert (N) needs the key absent and leaves (present, its value); an update (U) needs it present
+// and leaves (present, its value); a delete that removed (D) needs it present and leaves it
+// absent.  Observers leave the state alone: a lookup that found value v needs (present, v); a
+// lookup that missed, a delete that found nothing and an insert that was not placed need the key
+// absent.  An observer can always go right after a write that produced its state (or first, for
+// the state before the launch), so an order exists iff the writes can be ordered: N and D
+// alternate starting from the state before, U only while present, every observed value is
+// written by some N or U (or was there before), and the last write leaves the final state.
+// Returns 1 when some order exists, 0 when none does.
+inline int serial_closed_form(const std::vector<SerialOp>& G, bool present, uint32_t value, bool fin_present,
+                              uint32_t fin_value) {
+    int64_t nN = 0, nU = 0, nD = 0;
+    bool absent_seen = false;
+    bool fin_by_u = false, fin_by_n = false;
+    std::vector<uint32_t> written, looked;
+    for (const SerialOp& o : G) {
+        switch (o.type) {
+            case 0:
+                if (o.ov != 0) return 0;
+                if (o.st == 0) {
+                    absent_seen = true;
+                } else if (o.st == 1 || o.st == 3) {
+                    ++nN;
+                    written.push_back(o.val);
+                    fin_by_n |= o.val == fin_value;
+                } else if (o.st == 2) {
+                    ++nU;
+                    written.push_back(o.val);
+                    fin_by_u |= o.val == fin_value;
+                } else {
+                    return 0;
+                }
+                break;
+            case 1:
+                if (o.st == 1) looked.push_back(o.ov);
+                else if (o.st == 0 && o.ov == 0) absent_seen = true;
+                else return 0;
+                break;
+            case 2:
+                if (o.ov != 0) return 0;
+                if (o.st == 1) ++nD;
+                else if (o.st == 0) absent_seen = true;
+                else return 0;
+                break;
+            case 3:
+                return 0;  // not decided by this form
+            default:
+                if (o.st != 0 || o.ov != 0) return 0;
+                break;
+        }
+    }
+    bool end_present;
+    if (!present) {
+        if (nN != nD && nN != nD + 1) return 0;
+        if (nU > 0 && nN == 0) return 0;
+        end_present = nN == nD + 1;
+    } else {
+        if (nD != nN && nD != nN + 1) return 0;
+        end_present = nD == nN;
+    }
+    if (end_present != fin_present) return 0;
+    if (absent_seen && present && nD == 0) return 0;
+    std::sort(written.begin(), written.end());
+    for (uint32_t v : looked)
+        if (!std::binary_search(written.begin(), written.end(), v) && !(present && value == v)) return 0;
+    if (fin_present) {
+        if (nN + nU == 0) return value == fin_value ? 1 : 0;
+        // the last write is a U carrying the final value, or the last N carrying it with every U
+        // in an earlier present stretch (the one before the launch, or one after another N)
+        if (!fin_by_u && !(fin_by_n && (nU == 0 || present || nN >= 2))) return 0;
+    }
+    return 1;
+}
+
+inline bool has_increment(const std::vector<SerialOp>& G) {
+    for (const SerialOp& o : G)
+        if (o.type == 3) return true;
+    return false;
+}
+
 }  // namespace
 
 extern "C" {
@@ -467,6 +648,140 @@ void hive_oracle_map_apply(void* h, const uint8_t* types, const uint32_t* keys, 
         status[i] = st;
         out_vals[i] = ov;
     }
+}
+
+// The per-key serialisation check of a run of concurrent launches (see SerialSearch).
+// ops: types / keys / vals with launch[i] = the index of the launch op i ran in; status /
+// out_vals: what the table under test returned; fin_keys / fin_vals: its contents after the run,
+// sorted by key.  The map holds the state before the run.  Key 0 is never stored, so its ops
+// must all report status 0.  A key whose ops all ran in one launch and include no increment is
+// decided by serial_closed_form, any other by the search.  Returns the number of keys with no
+// valid order (a key whose launch holds more than 63 of its ops, or whose search exceeds 2^22
+// steps, counts as one); *first_bad = the lowest op index of such a key.  When it returns 0 the
+// map holds the final state of every key the run touched.
+uint64_t hive_oracle_map_check_serial(void* h, const uint8_t* types, const uint32_t* keys, const uint32_t* vals,
+                                      const uint32_t* launch, uint64_t n, const uint8_t* status,
+                                      const uint32_t* out_vals, const uint32_t* fin_keys, const uint32_t* fin_vals,
+                                      uint64_t n_fin, uint64_t* first_bad) {
+    auto& m = ((ReplayMap*)h)->m;
+    std::vector<uint64_t> idx(n);
+    for (uint64_t i = 0; i < n; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+        if (keys[a] != keys[b]) return keys[a] < keys[b];
+        if (launch[a] != launch[b]) return launch[a] < launch[b];
+        return a < b;
+    });
+    uint64_t bad = 0;
+    if (first_bad) *first_bad = ~0ull;
+    std::vector<std::pair<uint32_t, std::pair<bool, uint32_t>>> finals;
+    std::vector<std::vector<SerialOp>> groups;
+    for (uint64_t s = 0; s < n;) {
+        const uint32_t k = keys[idx[s]];
+        uint64_t e = s;
+        uint64_t low = idx[s];
+        groups.clear();
+        while (e < n && keys[idx[e]] == k) {
+            const uint64_t i = idx[e];
+            low = std::min(low, i);
+            if (e == s || launch[i] != launch[idx[e - 1]]) groups.emplace_back();
+            groups.back().push_back(SerialOp{types[i], vals ? vals[i] : 0u, status[i], out_vals ? out_vals[i] : 0u});
+            ++e;
+        }
+        bool ok = true;
+        for (const auto& G : groups) ok = ok && G.size() <= 63;
+        bool fin_present = false;
+        uint32_t fin_value = 0;
+        if (k != 0) {
+            const uint32_t* it = std::lower_bound(fin_keys, fin_keys + n_fin, k);
+            if (it != fin_keys + n_fin && *it == k) {
+                fin_present = true;
+                fin_value = fin_vals[it - fin_keys];
+            }
+        }
+        bool present = false;
+        uint32_t value = 0;
+        if (k != 0) {
+            auto mt = m.find(k);
+            if (mt != m.end()) {
+                present = true;
+                value = mt->second;
+            }
+        }
+        if (ok && groups.size() == 1 && !has_increment(groups[0])) {
+            ok = serial_closed_form(groups[0], present, value, fin_present, fin_value) == 1;
+        } else if (ok) {
+            SerialSearch srch{&groups, fin_present, fin_value, 1ll << 22, {}};
+            ok = srch.run(0, 0, present, value);
+        }
+        if (!ok) {
+            ++bad;
+            if (first_bad && low < *first_bad) *first_bad = low;
+        } else if (k != 0) {
+            finals.push_back({k, {fin_present, fin_value}});
+        }
+        s = e;
+    }
+    if (!bad)
+        for (const auto& f : finals) {
+            if (f.second.first) m[f.first] = f.second.second;
+            else m.erase(f.first);
+        }
+    return bad;
+}
+
+// Self-test of the closed form against the search on random single-launch groups of up to
+// max_ops ops without increments (random results: mostly inconsistent, plus results of a random
+// order of the ops).  Returns the number of groups on which the two disagree.
+uint64_t hive_oracle_serial_selftest(uint64_t seed, uint64_t trials, int max_ops) {
+    uint64_t st = seed, disagree = 0;
+    auto rnd = [&](uint64_t m) { return sm64(st) % m; };
+    for (uint64_t t = 0; t < trials; ++t) {
+        const int m = 1 + (int)rnd((uint64_t)max_ops);
+        std::vector<SerialOp> G(m);
+        bool present = rnd(2), fin_present;
+        uint32_t value = 1 + (uint32_t)rnd(3), fin_value;
+        for (auto& o : G) {
+            o.type = (uint8_t)rnd(3);
+            o.val = 1 + (uint32_t)rnd(3);
+        }
+        if (rnd(2)) {  // results of one random order
+            std::vector<int> ord(m);
+            for (int i = 0; i < m; ++i) ord[i] = i;
+            for (int i = m - 1; i > 0; --i) std::swap(ord[i], ord[rnd((uint64_t)i + 1)]);
+            bool p = present;
+            uint32_t v = value;
+            for (int i : ord) {
+                SerialOp& o = G[i];
+                o.ov = 0;
+                if (o.type == 0) {
+                    o.st = p ? 2 : 1;
+                    p = true;
+                    v = o.val;
+                } else if (o.type == 1) {
+                    o.st = p;
+                    o.ov = p ? v : 0;
+                } else {
+                    o.st = p;
+                    p = false;
+                }
+            }
+            fin_present = p;
+            fin_value = p ? v : 0;
+        } else {  // arbitrary results
+            for (auto& o : G) {
+                o.st = (uint8_t)rnd(3);
+                o.ov = o.type == 1 && o.st == 1 ? 1 + (uint32_t)rnd(3) : 0;
+            }
+            fin_present = rnd(2);
+            fin_value = fin_present ? 1 + (uint32_t)rnd(3) : 0;
+        }
+        std::vector<std::vector<SerialOp>> groups{G};
+        SerialSearch srch{&groups, fin_present, fin_value, 1ll << 30, {}};
+        const bool a = srch.run(0, 0, present, value);
+        const bool b = serial_closed_form(G, present, value, fin_present, fin_value) == 1;
+        disagree += a != b;
+    }
+    return disagree;
 }
 
 // Writes the key->value set sorted by key; returns its size.
