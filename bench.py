@@ -12,7 +12,9 @@ find_host over hive_insert_host / hive_find_host) from pinned host buffers, with
 copies of keys/values/lookup keys and the device->host copies of statuses/found flags/values
 inside the timed region (the library overlaps them with the table work in 2^22-op chunks).
 `cpu_baseline` / `--impl reference` time the CPU port of the same algorithm
-(oracle/hive_oracle.cpp, std::thread on every host core) on a bounded sample.
+(oracle/hive_oracle.cpp, std::thread on every host core) on the same workload (about a second of
+CPU work per step); `--impl reference` also runs the reference's own GPU build for sm_100a beside
+this table on the same keys (`reference_gpu`).
 
 Multi-GPU (torchrun): each rank owns an independent table with its own keys (seed 7 + 1000*rank);
 there is no data-path collective, so scaling is weak.
@@ -62,7 +64,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-bucket ceiling probes")
-    ap.add_argument("--cpu-sample-log", type=int, default=24, help="log2 slots of the CPU-baseline sample")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip the A/B against the reference's own GPU build")
     ap.add_argument("--workload", choices=["bulk", "batched", "served", "resize"], default="bulk",
                     help="bulk: the headline (default); the others run one GPU and print their own line")
     ap.add_argument("--batches", type=int, default=4096, help="batched: number of mixed batches")
@@ -246,48 +249,103 @@ def pcie_bandwidth(dev, nbytes=256 << 20, reps=4):
     return out
 
 
-def cpu_baseline(args, threads=None):
-    """The CPU port of the same algorithm (oracle/hive_oracle.cpp) on every host core: a bounded
-    sample with the headline's LF and present fraction at 2^cpu_sample_log slots."""
-    import oracle
-    from hivehashtable_b200 import workload
+class CpuPort:
+    """The CPU port of the same algorithm (oracle/hive_oracle.cpp: same policy, 8-slot buckets,
+    CAS claims, depth-1 eviction, stash) on every host core, over the headline workload itself:
+    n inserts into 2^cap_log slots, then n lookups at the present fraction.  One step is about a
+    second of CPU work at 2^26 slots."""
 
-    threads = threads or oracle.host_threads()
-    cap = 1 << args.cpu_sample_log
-    n = int(args.lf * cap)
-    keys, vals, look = workload.bulk_workload(args.seed, n, args.present)
-    t = oracle.CpuTable(0 if args.policy == "Default2Hash" else 1, cap)
-    _, ti = t.insert(keys, vals, threads)
-    _, f, tf = t.find(look, threads)
-    del t
-    mops = 2 * n / (ti + tf) / 1e6
-    return {"value": round(mops, 2), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} inserts into 2^{args.cpu_sample_log} slots (LF {args.lf}) + {n} lookups "
-                      f"({args.present:.0%} present), std::thread x {threads}",
-            "insert_mops": round(n / ti / 1e6, 2), "lookup_mops": round(n / tf / 1e6, 2),
-            "seconds": round(ti + tf, 3)}
+    def __init__(self, args, threads=None):
+        import oracle
+        from hivehashtable_b200 import workload
+
+        self.oracle = oracle
+        self.threads = threads or oracle.host_threads()
+        self.cap = 1 << args.cap_log
+        self.n = int(args.lf * self.cap)
+        self.args = args
+        self.keys, self.vals, self.look = workload.bulk_workload(args.seed, self.n, args.present)
+
+    def step(self):
+        a = self.args
+        t = self.oracle.CpuTable(0 if a.policy == "Default2Hash" else 1, self.cap)
+        _, ti = t.insert(self.keys, self.vals, self.threads)
+        _, f, tf = t.find(self.look, self.threads)
+        failed = t.failed
+        del t
+        n = self.n
+        return {"value": round(2 * n / (ti + tf) / 1e6, 2), "unit": UNIT, "cores": self.threads, "kind": "port",
+                "sample": f"the full workload: {n:,} inserts into 2^{a.cap_log} slots (LF {a.lf}) + {n:,} lookups "
+                          f"({a.present:.0%} present), std::thread x {self.threads}",
+                "insert_mops": round(n / ti / 1e6, 2), "lookup_mops": round(n / tf / 1e6, 2),
+                "seconds": round(ti + tf, 3), "inserts_failed": int(failed), "found": int(f.sum())}
+
+
+def cpu_baseline(args, threads=None):
+    """One step of the CPU port over the headline workload (CpuPort)."""
+    return CpuPort(args, threads).step()
+
+
+def reference_gpu(args):
+    """The reference's own GPU build for sm_100a (oracle/_ref/libhive_ref_gpu.so, compiled from its
+    src/hive_dispatch.cu, src/hive_memory.cu, src/GPUTimer.cc) beside this table on the same keys,
+    each in a process of its own (oracle.ref_gpu_ab): at the headline size, and at 2^22 slots where
+    both place every key, so their per-op success flags can be compared one by one."""
+    import oracle.ref_gpu_ab as ab
+
+    if not ab.available():
+        return {"unavailable": "the reference's GPU build is absent (it is compiled only where the reference "
+                               "tree is present)"}
+    out = {"build": "reference src/hive_dispatch.cu + src/hive_memory.cu, nvcc -arch=sm_100a -O3, run unchanged",
+           "timing": "the reference's own cudaEvent pair around one kernel launch; this table: CUDA events around "
+                     "hive_insert (all its launches) and hive_find"}
+    for cap_log in (args.cap_log, 22):
+        try:
+            p = subprocess.run([sys.executable, "-m", "oracle.ref_gpu_ab", str(cap_log), str(args.lf),
+                                str(args.present)], capture_output=True, text=True, timeout=900, cwd=str(ROOT))
+            line = [ln for ln in p.stdout.splitlines() if ln.startswith("REF_AB ")]
+            if p.returncode != 0 or not line:
+                out[f"cap_2p{cap_log}"] = {"error": (p.stdout + p.stderr)[-400:]}
+                continue
+            r = json.loads(line[-1][7:])
+        except Exception as e:  # a failed reference run leaves the CPU arm's line intact
+            out[f"cap_2p{cap_log}"] = {"error": repr(e)[-400:]}
+            continue
+        out[f"cap_2p{cap_log}"] = {
+            "keys": r["n"], "reference_insert_ms": round(r["reference"]["insert_ms"], 4),
+            "reference_lookup_ms": round(r["reference"]["lookup_ms"], 4),
+            "hive_insert_ms": round(r["hive"]["insert_ms"], 4), "hive_lookup_ms": round(r["hive"]["lookup_ms"], 4),
+            "speedup_insert": round(r["speedup_insert"], 2), "speedup_lookup": round(r["speedup_lookup"], 2),
+            "reference_unplaced": r["n"] - r["reference"]["inserted"], "hive_unplaced": r["n"] - r["hive"]["inserted"],
+            "insert_flags_equal": r["insert_flags_equal"], "lookup_flags_equal": r["lookup_flags_equal"]}
+    return out
 
 
 def run_reference(args, rank, world):
     line = {"metric": METRIC, "impl": "reference", "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic"}
+            "dtype": "u32", "data": "synthetic (splitmix64 seeded uint32 keys/values)"}
     if rank != 0:
         return None
+    port = CpuPort(args)
     for _ in range(args.warmup):
-        cpu_baseline(args)
+        port.step()
     vals, secs = [], 0.0
     cb = None
     for _ in range(args.steps):
-        cb = cpu_baseline(args)
+        cb = port.step()
         vals.append(cb["value"])
         secs += cb["seconds"]
-    v = statistics.median(vals)
+    v = round(statistics.median(vals), 2)
     cb["value"] = v
     line.update({"value": v, "ms_per_step": round(secs / args.steps * 1e3, 3),
-                 "config": workload_config(args, world, note="CPU port of the reference algorithm, bounded sample"),
+                 "config": workload_config(args, world),
+                 "what": "the reference has no CPU implementation of this path: the CPU port of its algorithm "
+                         "(oracle/hive_oracle.cpp) on every host core; its own GPU build is under reference_gpu",
                  "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
                                              "d2h_bytes_per_step": 0}})
+    if not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu(args)
     return line
 
 
@@ -467,7 +525,7 @@ def run_resize(args, dev):
     return out
 
 
-def workload_config(args, world, note=None):
+def workload_config(args, world):
     cap = 1 << args.cap_log
     n = int(args.lf * cap)
     d = {"workload": f"bulk insert of {n:,} unique uint32 keys into 2^{args.cap_log} slots (LF {args.lf}) then "
@@ -476,8 +534,6 @@ def workload_config(args, world, note=None):
          "policy": args.policy, "seed": args.seed,
          "l2": f"inputs larger than L2 (table {cap * 8 >> 20} MiB, each key array {n * 4 / 1e6:.0f} MB); no flush",
          "parallelism": f"replicas: {world} independent table(s), one per GPU"}
-    if note:
-        d["note"] = note
     return d
 
 

@@ -1,11 +1,14 @@
-"""Subprocess worker for tests/test_gpu_reference_ab.py.
+"""TEST INFRASTRUCTURE: A/B of the reference's own GPU build against the B200 table.
 
-Runs the reference's own GPU build (oracle/_ref/libhive_ref_gpu.so) and the B200 table on the same
-seeded keys and prints one JSON line with per-op flag agreement and both sides' kernel times.
-Isolated in its own process because the reference reserves ~60 % of free HBM when it loads and
-ends the process on any CUDA error.
+Runs the reference's GPU path (oracle/_ref/libhive_ref_gpu.so: its src/hive_dispatch.cu,
+src/hive_memory.cu and src/GPUTimer.cc compiled unchanged for sm_100a by oracle/build.py) and the
+B200 table on the same seeded keys (splitmix64 seed 7, value = key + 1 as the reference's kernels
+set it, include/hive_kernels.cuh:238) and prints one JSON line, prefixed "REF_AB ", with per-op
+success-flag agreement and both sides' kernel times.  Used by tests/test_gpu_reference_ab.py and by
+bench.py's reference arm.  Run it in a process of its own: the reference reserves ~60 % of free HBM
+when it loads and ends the process on any CUDA error.
 
-usage: python tests/ref_ab_worker.py CAP_LOG LOAD_FACTOR PRESENT_FRACTION
+usage: python -m oracle.ref_gpu_ab CAP_LOG LOAD_FACTOR PRESENT_FRACTION
 """
 import ctypes
 import json
@@ -15,7 +18,13 @@ from pathlib import Path
 import numpy as np
 
 ROOT = Path(__file__).resolve().parents[1]
-sys.path.insert(0, str(ROOT))
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+LIB = Path(__file__).resolve().parent / "_ref" / "libhive_ref_gpu.so"
+
+
+def available() -> bool:
+    return LIB.exists()
 
 
 def main():
@@ -57,7 +66,7 @@ def main():
     torch.cuda.empty_cache()
 
     # -- the reference's own GPU build --
-    lib = ctypes.CDLL(str(ROOT / "oracle" / "_ref" / "libhive_ref_gpu.so"))
+    lib = ctypes.CDLL(str(LIB))
     P, S, I, D = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
     lib.ref_bulk_insert.argtypes = [P, S, S, I, I, D, P]
     lib.ref_lookup.argtypes = [P, S, P, S, S, I, D, P]

@@ -18,8 +18,8 @@ ROOT = Path(__file__).resolve().parents[1]
 def test_reference_gpu_same_flags(cuda, cap_log, lf, present):
     if not (oracle.REF_DIR / "libhive_ref_gpu.so").exists():
         pytest.skip("reference GPU build not present (needs the reference tree at build time)")
-    p = subprocess.run([sys.executable, str(ROOT / "tests" / "ref_ab_worker.py"), str(cap_log), str(lf), str(present)],
-                       capture_output=True, text=True, timeout=900)
+    p = subprocess.run([sys.executable, "-m", "oracle.ref_gpu_ab", str(cap_log), str(lf), str(present)],
+                       capture_output=True, text=True, timeout=900, cwd=str(ROOT))
     line = [ln for ln in p.stdout.splitlines() if ln.startswith("REF_AB ")]
     assert p.returncode == 0 and line, p.stdout[-3000:] + p.stderr[-3000:]
     r = json.loads(line[-1][7:])
