@@ -517,10 +517,20 @@ __device__ __forceinline__ int nth_bit(uint32_t m, int n) {
     return pos;
 }
 
+// Slot masks of one half-bucket S for key k, placed for half h: bits 4h..4h+3 the free slots,
+// bits 8+4h..11+4h the slots holding k.
+__device__ __forceinline__ uint32_t half_masks(const Sector& S, uint32_t k, unsigned h) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) m |= ((uint32_t)(S.s[q] == 0ull) << q) | ((uint32_t)(key_of(S.s[q]) == k) << (8 + q));
+    return m << (4 * h);
+}
+
 // Every lane of a converged warp calls it.  A lane with `need` gets bucket b's slot masks: bits
 // 0-7 the free slots, bits 8-15 the slots holding k (k != 0, so a free slot never matches); other
 // lanes get 0.  In each round lane l loads half (l & 1) of the bucket of the (l >> 1)-th needing
-// lane not yet served, so up to 16 buckets take one load instruction.
+// lane not yet served, so up to 16 buckets take one load instruction.  (Issuing both rounds'
+// loads before using either was measured no faster and needs 8 more registers.)
 __device__ __forceinline__ uint32_t warp_bucket_masks(const u64* __restrict__ slots, bool need, uint32_t b,
                                                       uint32_t k) {
     const unsigned lane = lane_id();
@@ -537,16 +547,62 @@ __device__ __forceinline__ uint32_t warp_bucket_masks(const u64* __restrict__ sl
         if (owner >= 0) {
             Sector S;
             load_sector(slots + (size_t)ob * kSlots + 4 * (lane & 1), S);
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                m |= ((uint32_t)(S.s[q] == 0ull) << q) | ((uint32_t)(key_of(S.s[q]) == ok) << (8 + q));
-            m <<= 4 * (lane & 1);
+            m = half_masks(S, ok, lane & 1u);
         }
         m |= __shfl_xor_sync(0xffffffffu, m, 1);
         const uint32_t got = __shfl_sync(0xffffffffu, m, (int)((2 * rank) & 31u));
         if (need && (int)(rank >> 4) == r) out = got;
     }
     return out;
+}
+
+// warp_bucket_masks over two buckets per needing lane at once (both halves of both in the same
+// rounds): *ma and *mb receive the masks of buckets a and b, and keys_a the eight keys of a.
+__device__ __forceinline__ void warp_two_buckets(const u64* __restrict__ slots, bool need, uint32_t a, uint32_t b,
+                                                 uint32_t k, uint32_t (&keys_a)[kSlots], uint32_t* ma,
+                                                 uint32_t* mb) {
+    const unsigned lane = lane_id();
+    const unsigned h = lane & 1u;
+    const unsigned all = __ballot_sync(0xffffffffu, need);
+    const unsigned rank = __popc(all & ((1u << lane) - 1u));
+    const int rounds = (__popc(all) + 15) >> 4;
+    const int from = (int)((2 * rank) & 31u);
+    *ma = *mb = 0;
+    for (int r = 0; r < rounds; ++r) {
+        const int owner = nth_bit(all, 16 * r + (int)(lane >> 1));
+        const int src = owner < 0 ? 0 : owner;
+        const uint32_t oa = __shfl_sync(0xffffffffu, a, src);
+        const uint32_t ob = __shfl_sync(0xffffffffu, b, src);
+        const uint32_t ok = __shfl_sync(0xffffffffu, k, src);
+        uint32_t xa = 0, xb = 0, kk[4] = {0, 0, 0, 0};
+        if (owner >= 0) {
+            Sector SA, SB;
+            load_sector(slots + (size_t)oa * kSlots + 4 * h, SA);
+            load_sector(slots + (size_t)ob * kSlots + 4 * h, SB);
+            xa = half_masks(SA, ok, h);
+            xb = half_masks(SB, ok, h);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) kk[q] = key_of(SA.s[q]);
+        }
+        xa |= __shfl_xor_sync(0xffffffffu, xa, 1);
+        xb |= __shfl_xor_sync(0xffffffffu, xb, 1);
+        const uint32_t ga = __shfl_sync(0xffffffffu, xa, from);
+        const uint32_t gb = __shfl_sync(0xffffffffu, xb, from);
+        const bool mine = need && (int)(rank >> 4) == r;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t lo = __shfl_sync(0xffffffffu, kk[q], from);
+            const uint32_t hi = __shfl_sync(0xffffffffu, kk[q], from + 1);
+            if (mine) {
+                keys_a[q] = lo;
+                keys_a[4 + q] = hi;
+            }
+        }
+        if (mine) {
+            *ma = ga;
+            *mb = gb;
+        }
+    }
 }
 
 // Find k in bucket b using its tag word T: reads only the sectors holding a matching fingerprint.
@@ -1213,6 +1269,104 @@ __device__ __forceinline__ uint8_t insert_deferred_one(const Table& t, uint32_t 
         if (st) return st;
     }
     return insert_locked_path<P>(t, k, kv, b0, b1);
+}
+
+// The locked path of a second-pass insert into a table without holes, with every lane of the
+// warp in step: each lane (with `on`) takes its op through one fixed sequence -- one attempt at
+// H0's lock; H0 and H1 read together, one request per bucket shared by a lane pair
+// (warp_two_buckets), and H0's stash flag; an update if the key is already there (placed by an
+// earlier op of the same key, whose insert holds the same lock); else the H1 and full hint of
+// four slots of H0 at a time; the masks of the first open victim's bucket (one shared request)
+// and the victim's slot; the copy of the victim there, then the key over the victim -- so the
+// lanes' dependent memory accesses overlap instead of running one divergent path after another.
+// (Per-lane whole-bucket reads, two requests per bucket, measured slower here.)  Returns kStInserted / kStUpdated, or kStDefer for an op that meets anything else
+// (lock taken, H0's stash flagged, no open victim, a victim bucket found full, a lost CAS, a slot
+// free against expectation): such an op holds no lock and has changed nothing, and is handed on
+// to a pass that runs the general locked path.  Only for launches without tag upkeep
+// (kFlagUntagged).
+//
+// Without holes a bucket the first pass found full stays full, and every change to a key's
+// entries is made under that key's H0 lock, so under H0's lock the victim's slot cannot change
+// between the copy and the overwrite, and an existing copy of k is updated by an exchange.
+template <int P>
+__device__ __forceinline__ uint8_t insert_locked_converged(const Table& t, bool on, uint32_t k, uint32_t v) {
+    const u64 kv = pack(k, v);
+    const uint32_t b0 = on ? bucket_addr(t, Policy<P>::h0(k)) : 0u;
+    const uint32_t b1 = on ? bucket_addr(t, Policy<P>::h1(k)) : 0u;
+    if (on) count(t, kCtrSlowPath);
+    const bool locked = on && lock_byte_try(t, b0);
+    if (on && !locked) count(t, kCtrLockWaits);
+    u64* B0p = t.slots + (size_t)b0 * kSlots;
+    // H0 (its keys and masks) and H1 (masks) in shared requests, and the stash flag; the victim's
+    // whole slot is read again, an L2 hit, once it is chosen
+    const bool stashed = locked && stash_flag(t, b0);
+    uint32_t keys[kSlots], m0, m1;
+    warp_two_buckets(t.slots, locked, b0, b1, k, keys, &m0, &m1);
+    if (b1 == b0) m1 = 0u;  // no second bucket: neither room nor a copy there
+    uint8_t st = kStDefer;
+    bool evict = false;
+    if (locked) {
+        if (m0 >> 8) {
+            atomicExch(B0p + (__ffs(m0 >> 8) - 1), kv);
+            st = kStUpdated;
+        } else if ((m1 >> 8) && b1 != b0) {
+            atomicExch(t.slots + (size_t)b1 * kSlots + (__ffs(m1 >> 8) - 1), kv);
+            st = kStUpdated;
+        } else {
+            // a flagged stash may hold k (its entries change only under H0's lock): general path
+            evict = !(m0 & 0xFFu) && !(m1 & 0xFFu) && !stashed;
+        }
+    }
+    // the first open victim: H1 and full hint of four slots at a time, the next four only when
+    // none of the first is open
+    const int limit = t.max_evictions < (uint32_t)kSlots ? (int)t.max_evictions : kSlots;
+    uint32_t alt = 0;
+    int jv = -1;
+#pragma unroll 1
+    for (int g = 0; evict && jv < 0 && g < limit; g += kEvictGroup) {
+        uint32_t open = 0;
+#pragma unroll
+        for (int q = 0; q < kEvictGroup; ++q) {
+            uint32_t kq = keys[0];
+#pragma unroll
+            for (int j = 1; j < kSlots; ++j)
+                if (j == g + q) kq = keys[j];
+            const uint32_t a = bucket_addr(t, Policy<P>::h1(kq));
+            if (g + q < limit && a != b0 && !((__ldcg(t.full_bits + (a >> 5)) >> (a & 31)) & 1u)) open |= 1u << q;
+        }
+        if (open) {
+            jv = g + __ffs(open) - 1;
+            uint32_t kj = keys[0];
+#pragma unroll
+            for (int j = 1; j < kSlots; ++j)
+                if (j == jv) kj = keys[j];
+            alt = bucket_addr(t, Policy<P>::h1(kj));
+        }
+    }
+    const bool try_alt = evict && jv >= 0;
+    const u64 vkv = try_alt ? ld_relaxed_u64(B0p + jv) : 0ull;
+    const uint32_t ma = warp_bucket_masks(t.slots, try_alt, alt, 0xFFFFFFFFu);
+    if (try_alt) {
+        const uint32_t e = ma & 0xFFu;
+        if (!e) {
+            mark_full(t, alt);
+        } else {
+            u64* Ap = t.slots + (size_t)alt * kSlots;
+            const int d = __ffs(e) - 1;
+            if (cas64(Ap + d, 0ull, vkv) == 0ull) {
+                if (__popc(e) == 1) mark_full(t, alt);
+                // the victim is now in both places; the key takes its H0 slot
+                if (cas64(B0p + jv, vkv, kv) == vkv) {
+                    count(t, kCtrEvictions);
+                    st = kStInserted;
+                } else if (cas64(Ap + d, vkv, 0ull) == vkv) {
+                    mark_not_full(t, alt);
+                }
+            }
+        }
+    }
+    if (locked) unlock_bucket(t, b0);
+    return st;
 }
 
 // ---------------------------------------------------------------------------------------------

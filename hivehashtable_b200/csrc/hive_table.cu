@@ -209,8 +209,8 @@ __global__ void __launch_bounds__(kBlock, (kDefer && hive::mode_base(kMode) == h
     uint8_t st = hive::kStFail;
     if constexpr (kDefer && hive::mode_base(kMode) == hive::kModeMono && (kMode & hive::kModeUntagged) &&
                   !(kMode & hive::kModePrimary)) {
-        // Bulk first pass: each bucket read is one request shared by a lane pair (every lane of
-        // the warp takes part in both rounds, so nothing here returns early).
+        // Bulk first pass, one op per thread: each bucket read is one request shared by a lane
+        // pair (every lane of the warp takes part, so nothing here returns early).
         const uint32_t k = active ? __ldcs(keys + i) : 0u;
         const uint32_t v = active ? __ldcs(vals + i) : 0u;
         const bool live = k != 0u;
@@ -296,6 +296,50 @@ __global__ void __launch_bounds__(kBlock, 4) k_insert_deferred(hive::Table t, co
     }
 }
 
+// The general locked path out of line, for the rare op of the converged pass below that finds
+// the third-pass queue full (kFlagResumed: it was counted on the slow path already).
+template <int P>
+__device__ __noinline__ uint8_t insert_deferred_general(const hive::Table& t, uint32_t k, uint32_t v) {
+    hive::Table tr = t;
+    tr.flags = (t.flags & ~hive::kFlagHandOn) | hive::kFlagResumed;
+    return hive::insert_deferred_one<P>(tr, k, v);
+}
+
+// Second pass of a bulk insert into a table without holes and without tag upkeep, with the
+// third-pass queue present: every lane of a warp takes its queued op through the warp-converged
+// locked path (insert_locked_converged); ops it does not finish go to the third-pass queue, which
+// the general pass (k_insert_deferred) finishes.  Statuses: kStInserted is already written
+// (provisional), an update writes kStUpdated, a handed-on op's status is written by the third pass.
+template <int P>
+__global__ void __launch_bounds__(kBlock, 4) k_insert_converged(hive::Table t, uint8_t* __restrict__ status, Defer d) {
+    const u64 n = *d.n;
+    const u64 cnt = n < d.cap ? n : d.cap;
+    const u64 stride = (u64)gridDim.x * kBlock;
+    const unsigned lane = threadIdx.x & 31;
+    for (u64 j0 = (u64)blockIdx.x * kBlock + (threadIdx.x & ~31u); j0 < cnt; j0 += stride) {
+        const u64 j = j0 + lane;
+        const bool active = j < cnt;
+        const u64 e = active ? __ldcs(d.kv + j) : 0ull;
+        uint8_t st = hive::insert_locked_converged<P>(t, active, hive::key_of(e), hive::val_of(e));
+        const bool hand_on = active && st == hive::kStDefer;
+        const unsigned m = __ballot_sync(0xffffffffu, hand_on);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            u64 base = 0;
+            if ((int)lane == leader) base = atomicAdd(d.sn, (u64)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            const u64 pos = base + __popc(m & ((1u << lane) - 1u));
+            if (hand_on && pos < d.scap) {
+                d.sq[pos] = __ldcs(d.q + j);
+                d.skv[pos] = e;
+            } else if (hand_on) {
+                st = insert_deferred_general<P>(t, hive::key_of(e), hive::val_of(e));
+            }
+        }
+        if (status && active && st != hive::kStInserted && st != hive::kStDefer) status[__ldcs(d.q + j)] = st;
+    }
+}
+
 // The second pass and, for ops it handed on, the third.
 template <int P>
 void launch_second_pass(unsigned grid, cudaStream_t s, const hive::Table& t, const uint32_t* keys,
@@ -306,7 +350,10 @@ void launch_second_pass(unsigned grid, cudaStream_t s, const hive::Table& t, con
     }
     hive::Table t2 = t;
     if (d.sq) t2.flags |= hive::kFlagHandOn;
-    k_insert_deferred<P, true><<<grid, kBlock, 0, s>>>(t2, keys, vals, status, d);
+    if (d.sq && !d.permute && (t.flags & hive::kFlagUntagged) && !(t.flags & (hive::kFlagHoles | hive::kFlagPrimaryFirst)))
+        k_insert_converged<P><<<grid, kBlock, 0, s>>>(t2, status, d);
+    else
+        k_insert_deferred<P, true><<<grid, kBlock, 0, s>>>(t2, keys, vals, status, d);
     if (!d.sq) return;
     Defer d3{d.sq, d.sn};
     d3.kv = d.skv;
