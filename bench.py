@@ -174,7 +174,7 @@ def random_bucket_ceiling(dev, table_bytes):
     import torch
     from hivehashtable_b200 import build as pbuild
 
-    lib = ctypes.CDLL(str(pbuild.LIB / "libhive_probe.so"))
+    lib = ctypes.CDLL(str(pbuild.build_probe()))
     f = lib.hive_probe_random_buckets
     f.restype = ctypes.c_int
     f.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64,
@@ -187,6 +187,7 @@ def random_bucket_ceiling(dev, table_bytes):
              ("read32_table", table_bytes, 3, 32), ("read64_cas_table", table_bytes, 1, 96),
              ("cas_only_table", table_bytes, 5, 32), ("read32_cas_table", table_bytes, 6, 64),
              ("read64x2_table", table_bytes, 2, 128), ("read64x2_indep_table", table_bytes, 4, 128),
+             ("read64_pair_table", table_bytes, 7, 64), ("read64_pair_cas_table", table_bytes, 8, 96),
              ("read64_32MiB_l2", 32 << 20, 0, 64), ("read64_cas_32MiB_l2", 32 << 20, 1, 96),
              ("cas_only_32MiB_l2", 32 << 20, 5, 32)]
     for name, size, mode, bpo in cases:
@@ -699,10 +700,11 @@ def main():
                         "algorithmic_bytes": kd["bytes"], "ms_per_launch": round(kd["ms"], 4),
                         "mops": round(kd["ops"] / kd["ms"] / 1e3, 1)}
         if ceiling:
-            # the same ops at the probe's raw access rate: insert = one bucket read + CAS; lookup =
+            # the same ops at the probe's raw access rate: insert = one bucket read (one request
+            # shared by a lane pair, as the first pass reads) + CAS; lookup =
             # one random 32 B sector per present key (fingerprint words are L2 hits and an absent
             # key reads no slot)
-            ins_ceiling = ceiling["read64_cas_table"]["gops"]
+            ins_ceiling = ceiling["read64_pair_cas_table"]["gops"]
             p = max(args.present, 1e-9)
             look_ceiling = ceiling["read32_table"]["gops"] / p
             rl["k_insert"]["frac_of_probe_ops"] = round(rl["k_insert"]["mops"] / 1e3 / ins_ceiling, 4)

@@ -4,6 +4,8 @@ Outputs (git-ignored, shipped with the source tree):
   hivehashtable_b200/lib/libhive_b200.so     kernels + the C ABI of include/hive_c.h
   hivehashtable_b200/lib/libhive_compat.so   the reference's C++ API on top of the C ABI
   hivehashtable_b200/lib/libhive_workload.so seeded workload generator (host C++)
+  hivehashtable_b200/lib/libhive_serve.so    the served request loop (host C++)
+and, for bench.py only (build_probe), lib/libhive_probe.so: the random-access ceiling probes.
 
 Run as ``python -m hivehashtable_b200.build`` or through ``__graft_entry__.build()``.
 """
@@ -81,6 +83,8 @@ def build_compat(force: bool = False) -> Path:
 
 
 def build_probe(force: bool = False) -> Path:
+    """bench.py's random-access probes (csrc/hive_probe.cu): a measurement helper of the
+    benchmark, not part of the library; built on demand by bench.py."""
     out = LIB / "libhive_probe.so"
     src = CSRC / "hive_probe.cu"
     if force or _stale(out, [src]):
@@ -103,7 +107,7 @@ def build_serve(force: bool = False) -> Path:
 
 
 def build_all(force: bool = False) -> list[Path]:
-    outs = [build_core(force), build_workload(force), build_probe(force), build_serve(force)]
+    outs = [build_core(force), build_workload(force), build_serve(force)]
     if (CSRC / "hive_compat.cpp").exists():
         outs.append(build_compat(force))
     return outs

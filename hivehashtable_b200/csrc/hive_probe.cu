@@ -14,6 +14,10 @@
 //   mode 4  read two random 64 B buckets per thread, both addresses known up front
 //   mode 5  CAS 8 B in a random bucket with no read before it (value unchanged)
 //   mode 6  read the random slot's 32 B sector, then CAS 8 B in it (value unchanged)
+//   mode 7  read one random 64 B bucket per thread as one request shared by a lane pair (lane l
+//           loads half l & 1 of the buckets of lanes 2(l >> 1)... : each thread's bucket is read
+//           by two lanes, half each, in one of two load instructions per warp)
+//   mode 8  mode 7, then CAS 8 B in the bucket (value unchanged)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -98,6 +102,37 @@ __global__ void __launch_bounds__(256) k_probe(unsigned long long* buf, uint64_t
     if (acc == 0x9e3779b97f4a7c15ull) *sink = acc;  // keeps the loads live; practically never taken
 }
 
+// Modes 7 and 8: in round r lane l reads half (l & 1) of the bucket of lane 16r + (l >> 1), so one
+// warp instruction covers 16 buckets with one two-sector request each.  n must be a multiple of
+// 256 (every lane of every warp takes part in the shuffles).
+template <int kMode>
+__global__ void __launch_bounds__(256) k_probe_pair(unsigned long long* buf, uint64_t nb, uint64_t seed,
+                                                    unsigned long long* sink) {
+    const uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t b = mix64(i ^ seed) % nb;
+    unsigned long long acc = 0, mine = 0;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const uint64_t bb = __shfl_sync(0xffffffffu, b, 16 * r + (int)(lane >> 1));
+        unsigned long long v[4];
+        asm volatile("ld.relaxed.gpu.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                     : "=l"(v[0]), "=l"(v[1]), "=l"(v[2]), "=l"(v[3])
+                     : "l"(buf + bb * 8 + (lane & 1) * 4)
+                     : "memory");
+        unsigned long long x = v[0] ^ v[1] ^ v[2] ^ v[3];
+        x ^= __shfl_xor_sync(0xffffffffu, x, 1);
+        const unsigned long long got = __shfl_sync(0xffffffffu, x, (int)((2 * lane) & 31u));
+        if ((int)(lane >> 4) == r) mine = got;
+    }
+    acc = mine;
+    if (kMode == 8) {
+        const int j = (int)(i & 7);
+        acc ^= atomicCAS(buf + b * 8 + j, 0ull, 0ull);  // the insert's claim of a free slot
+    }
+    if (acc == 0x9e3779b97f4a7c15ull) *sink = acc;  // keeps the loads live; practically never taken
+}
+
 }  // namespace
 
 extern "C" {
@@ -105,7 +140,8 @@ extern "C" {
 // buf: device buffer of nb 64-byte buckets; n: buckets read (threads).  Returns a cudaError_t.
 __attribute__((visibility("default"))) int hive_probe_random_buckets(void* buf, uint64_t nb, uint64_t n, int mode,
                                                                       uint64_t seed, void* sink, void* stream) {
-    if (!buf || !nb || !sink || mode < 0 || mode > 6) return (int)cudaErrorInvalidValue;
+    if (!buf || !nb || !sink || mode < 0 || mode > 8) return (int)cudaErrorInvalidValue;
+    if (mode >= 7 && n % 256) return (int)cudaErrorInvalidValue;
     if (!n) return 0;
     const unsigned grid = (unsigned)((n + 255) / 256);
     cudaStream_t s = (cudaStream_t)stream;
@@ -117,7 +153,9 @@ __attribute__((visibility("default"))) int hive_probe_random_buckets(void* buf, 
     else if (mode == 3) k_probe<3><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
     else if (mode == 4) k_probe<4><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
     else if (mode == 5) k_probe<5><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
-    else k_probe<6><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else if (mode == 6) k_probe<6><<<grid, 256, 0, s>>>(p, nb, n, seed, k);
+    else if (mode == 7) k_probe_pair<7><<<grid, 256, 0, s>>>(p, nb, seed, k);
+    else k_probe_pair<8><<<grid, 256, 0, s>>>(p, nb, seed, k);
     return (int)cudaGetLastError();
 }
 

@@ -5,9 +5,10 @@
   oracle/_ref/hash_kat_uhf            reference UniformHashFunction hash_function.cu (plain-C hash2)
   oracle/_ref/libhive_ref_hashdev.so  reference device hash policies, sm_100a
 
-The reference is compiled directly from its sources where they lie (REFERENCE_ROOT, default
-/root/reference); nothing is copied into this repository and the reference's own build system is
-not used.  Outputs under oracle/_ref/ are git-ignored but travel with the source tree, so the GPU
+The reference is compiled directly from its sources where they lie (REFERENCE_ROOT: the
+HIVE_REFERENCE_ROOT environment variable, else a directory named `reference` beside this
+repository); nothing is copied into this repository and the reference's own build system is not
+used.  Outputs under oracle/_ref/ are git-ignored but travel with the source tree, so the GPU
 tests can use the prebuilt reference library where the reference tree is absent.
 """
 from __future__ import annotations
@@ -21,7 +22,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "lib"
 REF_OUT = HERE / "_ref"
-REFERENCE_ROOT = Path(os.environ.get("HIVE_REFERENCE_ROOT", "/root/reference"))
+REFERENCE_ROOT = Path(os.environ.get("HIVE_REFERENCE_ROOT", str(HERE.parents[1] / "reference")))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
