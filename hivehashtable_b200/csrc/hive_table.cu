@@ -78,7 +78,7 @@ struct hive_table {
     void* rbuf = nullptr;         // region-ordering buffers (13 bytes per op of the largest batch)
     uint64_t rcap = 0;
     int num_sms = 148;
-    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1, 1};  // HIVE_TUNE_* knobs
+    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1, 1, 1};  // HIVE_TUNE_* knobs
     bool tags_valid = true;  // the tag words match the slots (a zeroed table's do)
     void* ovf = nullptr;     // shrink: overflow entries of one merge step (kept between calls)
     size_t ovf_cap = 0;      // entries
@@ -93,6 +93,65 @@ struct hive_table {
 namespace {
 
 inline uint64_t num_buckets(const hive_table* h) { return (uint64_t)h->t.n_lo + h->t.split; }
+
+// ---- L2 persistence window (HIVE_TUNE_L2_WINDOW) ------------------------------------------------
+// A table whose memory fits in L2 (126 MB on B200; the persisting part of it is a per-process
+// limit, reserved here the first time a window is used on a device) is kept there against the
+// streaming inputs and outputs of its batches: for the duration of a call, the caller's stream
+// carries an access-policy window over the table's memory block with persisting hits, and the
+// stream's previous window is put back when the call has queued its launches.
+constexpr int kMaxWindowDevices = 64;
+size_t g_persist_reserved[kMaxWindowDevices] = {};
+std::mutex g_persist_mutex;
+
+struct L2Window {
+    cudaStream_t s = nullptr;
+    bool active = false;
+    cudaStreamAttrValue prev{};
+
+    L2Window(const hive_table* h, cudaStream_t stream) : s(stream) {
+        const int64_t mode = h->tune[HIVE_TUNE_L2_WINDOW];
+        if (mode == 0 || h->device < 0 || h->device >= kMaxWindowDevices) return;
+        int max_persist = 0, max_window = 0;
+        // a failed query or setting leaves the call without a window (and clears its error)
+        if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, h->device) != cudaSuccess ||
+            cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, h->device) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        if (max_persist <= 0 || max_window <= 0) return;
+        const size_t bytes = h->block_bytes;
+        if (mode == 1 && bytes > (size_t)max_persist) return;
+        {
+            std::lock_guard<std::mutex> lock(g_persist_mutex);
+            size_t& reserved = g_persist_reserved[h->device];
+            const size_t want = std::min(bytes, (size_t)max_persist);
+            if (reserved < want) {
+                if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+                    cudaGetLastError();
+                    return;
+                }
+                reserved = want;
+            }
+        }
+        if (cudaStreamGetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &prev) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        cudaStreamAttrValue w{};
+        w.accessPolicyWindow.base_ptr = h->block;
+        w.accessPolicyWindow.num_bytes = std::min(bytes, (size_t)max_window);
+        w.accessPolicyWindow.hitRatio =
+            (float)std::min(1.0, (double)max_persist / (double)w.accessPolicyWindow.num_bytes);
+        w.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        w.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        active = cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &w) == cudaSuccess;
+        if (!active) cudaGetLastError();
+    }
+    ~L2Window() {
+        if (active) cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &prev);
+    }
+};
 
 void set_geometry(hive_table* h, uint32_t level, uint32_t split) {
     h->level = level;
@@ -1465,6 +1524,7 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
     if (!keys || !values) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
     Defer d;
     int rc = prepare_defer(h, n, s, &d, true);
     if (rc) return rc;
@@ -1566,6 +1626,7 @@ int hive_find(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* values,
     if (!keys) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
     hive::Table tv;
     if (int vrc = table_view(h, s, &tv)) return vrc;
     if (use_regions(h, n, HIVE_TUNE_REGION_FIND)) {
@@ -1641,6 +1702,7 @@ int hive_insert_host(hive_table* h, const uint32_t* keys, const uint32_t* values
     DeviceGuard g(h->device);
     if (!g.ok) return HIVE_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
     Staging st;
     Defer d;
     int rc;
@@ -1676,6 +1738,7 @@ int hive_find_host(hive_table* h, const uint32_t* keys, uint64_t n, uint32_t* va
     DeviceGuard g(h->device);
     if (!g.ok) return HIVE_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
     Staging st;
     int rc = prepare_pipe(h, n, &st);
     if (rc) return rc;
@@ -1703,6 +1766,7 @@ int hive_erase(hive_table* h, const uint32_t* keys, uint64_t n, uint8_t* status,
     DeviceGuard g(h->device);
     h->t.flags |= hive::kFlagHoles;
     cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
     hive::Table tv;
     if (int vrc = table_view(h, s, &tv)) return vrc;
     HIVE_DISPATCH(k_erase, grid_for(n), kBlock, s, tv, keys, n, status);
@@ -1716,6 +1780,7 @@ int hive_apply_ops(hive_table* h, const uint8_t* types, const uint32_t* keys, co
     if (!types || !keys) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
     if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
     Defer d;
     int rc = prepare_defer(h, n, s, &d, true);
@@ -1742,6 +1807,7 @@ int hive_apply_batches(hive_table* h, const uint8_t* types, const uint32_t* keys
     if (threads_per_block % 32 || threads_per_block > 1024 || blocks_per_sm < 0) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
     if (!(hints & HIVE_HINT_NO_DELETES)) h->t.flags |= hive::kFlagHoles;
     Defer d;
     int rc = prepare_defer(h, max_batch_ops, s, &d);
@@ -1777,6 +1843,7 @@ int hive_apply_reference_ops(hive_table* h, const void* ops, uint64_t n, uint64_
     if (!ops || ((uintptr_t)ops & 15)) return HIVE_ERR_INVALID_ARG;
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
     // the holes flag first: the launch's view carries the flags
     if (!(hints & (HIVE_HINT_LOOKUPS_ONLY | HIVE_HINT_NO_DELETES))) h->t.flags |= hive::kFlagHoles;
     hive::Table tv;
@@ -1976,7 +2043,7 @@ int hive_debug_hold_lock(hive_table* h, uint64_t bucket, int held, void* stream)
 
 int hive_set_tuning(hive_table* h, int32_t key, int64_t value) {
     if (!valid_table(h) || key < 0 || key >= HIVE_NUM_TUNES) return HIVE_ERR_INVALID_ARG;
-    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0, 0}, hi[HIVE_NUM_TUNES] = {2, 1, 8, 8, 2, 2};
+    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0, 0, 0}, hi[HIVE_NUM_TUNES] = {2, 1, 8, 8, 2, 2, 2};
     if (value < lo[key] || value > hi[key]) return HIVE_ERR_INVALID_ARG;
     h->tune[key] = value;
     return HIVE_OK;

@@ -292,7 +292,13 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
                                         1 (default) while their words (8 bytes per bucket) fit
                                         64 MiB, i.e. up to 2^23 buckets, where they stay in L2;
                                         2 always                                                */
-#define HIVE_NUM_TUNES 6
+#define HIVE_TUNE_L2_WINDOW 6        /* L2 persistence window over the table's memory for the
+                                        table's launches (a stream access-policy window set for
+                                        the call and restored after it): 0 never; 1 (default)
+                                        when the table's memory fits the device's persisting-L2
+                                        limit (about 2^22 slots and below on B200); 2 always,
+                                        covering as much as the limit allows                    */
+#define HIVE_NUM_TUNES 7
 
 /* Set knob `key` to `value`.  HIVE_ERR_INVALID_ARG for an unknown key or a value out of range. */
 int hive_set_tuning(hive_table* t, int32_t key, int64_t value);

@@ -528,17 +528,30 @@ uint64_t hive_oracle_sm64(uint64_t* state) { return sm64(*state); }
 uint64_t hive_oracle_gen_keys(uint64_t seed, uint64_t n_present, uint64_t n_absent,
                               uint32_t* present, uint32_t* absent) {
     uint64_t state = seed;
-    std::unordered_set<uint32_t> seen;
-    seen.reserve((size_t)(n_present + n_absent) * 2);
+    // keys drawn so far: an open-addressing set (keys are never 0, so 0 marks a free cell) at
+    // most half full
+    uint64_t cells = 2;
+    while (cells < 2 * (n_present + n_absent)) cells <<= 1;
+    std::vector<uint32_t> seen(cells, 0u);
+    auto fresh = [&](uint32_t k) {
+        for (uint64_t c = (k * 0x9E3779B97F4A7C15ull) >> 20;; ++c) {
+            uint32_t& cell = seen[c & (cells - 1)];
+            if (cell == k) return false;
+            if (cell == 0u) {
+                cell = k;
+                return true;
+            }
+        }
+    };
     uint64_t i = 0;
     while (i < n_present) {
         uint32_t k = draw_key(state);
-        if (seen.insert(k).second) present[i++] = k;
+        if (fresh(k)) present[i++] = k;
     }
     i = 0;
     while (i < n_absent) {
         uint32_t k = draw_key(state);
-        if (seen.insert(k).second) absent[i++] = k;
+        if (fresh(k)) absent[i++] = k;
     }
     return state;
 }
@@ -583,6 +596,7 @@ uint64_t hive_oracle_map_size(void* h) { return ((ReplayMap*)h)->m.size(); }
 void hive_oracle_map_insert(void* h, const uint32_t* keys, const uint32_t* vals, uint64_t n,
                             const uint8_t* apply_mask, uint8_t* status) {
     auto& m = ((ReplayMap*)h)->m;
+    m.reserve(m.size() + n);
     for (uint64_t i = 0; i < n; ++i) {
         uint8_t st = 0;
         if (keys[i] != 0 && (!apply_mask || apply_mask[i])) {

@@ -88,9 +88,13 @@ def test_plain_bulk_small_config(cuda):
 
 
 @pytest.mark.parametrize("policy", POLICIES)
-@pytest.mark.parametrize("cap_log", [16, 20])
+@pytest.mark.parametrize("cap_log", [16, 20, 22, 24])
 @pytest.mark.parametrize("lf", [0.65, 0.80, 0.90, 0.95, 1.0])
 def test_bulk_sweep(cuda, policy, cap_log, lf):
+    """The bulk sweep (seed 7): capacity x load factor x both policies, every insert's status and
+    then n lookups at each present fraction compared op by op with the replay, and the full
+    key->value set.  2^22 and 2^24 slots are the sweep's own capacities; 2^26 is covered by
+    test_full_size_properties."""
     cap = 1 << cap_log
     n = int(lf * cap)
     keys, absent, st = oracle.gen_keys(7, n, n)
@@ -103,10 +107,10 @@ def test_bulk_sweep(cuda, policy, cap_log, lf):
             assert failed == 0, failed
         c = t.counters()
         assert c["failed"] == failed and c["error_bits"] == 0
+        placed = keys[ins != ST_FAIL]
         for p in (0.0, 0.25, 0.5, 0.75, 1.0):
-            npres = int(round(p * min(n, 1 << 14)))
-            nabs = min(n, 1 << 14) - npres
-            look, st = oracle.lookup_set(keys, absent, npres, nabs, st)
+            npres = int(round(p * n))
+            look, st = oracle.lookup_set(placed, absent, min(npres, placed.size), n - npres, st)
             _find_and_check(t, m, look)
         _assert_same_set(t, m)
 
@@ -567,15 +571,17 @@ def test_bucket_choice_matches_oracle(cuda):
                 np.testing.assert_array_equal(u32(b1), e1)
 
 
-def test_full_size_properties(cuda):
-    """Headline size: 2^26 slots at LF 0.9 (60,397,977 keys, seed 7).  Size-independent checks:
-    every insert succeeds, size equals n, every inserted key is found with its own value, absent
-    keys are missed, and the dump's key and value checksums equal the inputs'."""
+@pytest.mark.parametrize("policy", POLICIES)
+def test_full_size_properties(cuda, policy):
+    """Headline size: 2^26 slots at LF 0.9 (60,397,977 keys, seed 7), both policies.
+    Size-independent checks: every insert succeeds, size equals n, every inserted key is found
+    with its own value, absent keys are missed, and the dump's key and value checksums equal the
+    inputs'."""
     cap = 1 << 26
     n = int(0.9 * cap)
     keys, absent, _ = workload.gen_keys(7, n, 1 << 20)
     vals = workload.values_for(keys)
-    with HiveHashTable(cap) as t:
+    with HiveHashTable(cap, policy) as t:
         st = _np(t.insert(keys, vals))
         assert (st != ST_FAIL).all() and not (st == ST_UPDATED).any()
         assert t.size() == n
