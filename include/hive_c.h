@@ -294,10 +294,12 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
                                         2 always                                                */
 #define HIVE_TUNE_L2_WINDOW 6        /* L2 persistence window over the table's memory for the
                                         table's launches (a stream access-policy window set for
-                                        the call and restored after it): 0 never; 1 (default)
+                                        the call and restored after it): 0 (default) never; 1
                                         when the table's memory fits the device's persisting-L2
                                         limit (about 2^22 slots and below on B200); 2 always,
-                                        covering as much as the limit allows                    */
+                                        covering as much as the limit allows.  Measured at 2^22
+                                        slots (LF 0.9, L2 flushed between batches): 2% slower
+                                        with the window, so it is off unless asked for           */
 #define HIVE_NUM_TUNES 7
 
 /* Set knob `key` to `value`.  HIVE_ERR_INVALID_ARG for an unknown key or a value out of range. */
