@@ -5,12 +5,12 @@ submitted on any rank goes through one exchange step:
 
   1. owner of every op: a multiply-shift range reduction of an independent 32-bit mixer (not
      the table's own hash1/hash2, so each shard's bucket choice stays uniform);
-  2. ops grouped by owner (a stable sort), per-destination counts exchanged, then the
-     (type, key, value) records exchanged with all_to_all_single (NCCL over NVLink/NVSwitch on
-     GPUs, gloo on CPU);
+  2. ops grouped by owner (a stable sort), per-destination counts exchanged, then the packed
+     records -- key u32, value u32, type u8: 9 bytes per op -- exchanged with all_to_all_single
+     (NCCL over NVLink/NVSwitch on GPUs, gloo on CPU);
   3. each rank applies what it received to its shard (ops unordered within a batch, as locally);
-  4. the (status, value) results travel back with the reverse all_to_all_single and are put
-     back in submission order.
+  4. the results -- status u8, value u32: 5 bytes per op -- travel back with the reverse
+     all_to_all_single and are put back in submission order.
 
 All ranks must call apply() together, in the same order (the exchange is a collective).  The
 reference is single-GPU; this is the sharding it has no counterpart for.
@@ -52,9 +52,11 @@ class ShardedHiveTable:
         self.rank = dist.get_rank(group)
         self.device = device
         self.hints = hints
+        self.local = None
         if callable(local) and not hasattr(local, "apply"):
             self._apply = local
         else:
+            self.local = local
             self._apply = lambda t, k, v: local.apply(t, k, v, hints=self.hints)
 
     def _a2a(self, x: torch.Tensor, send_counts, recv_counts) -> torch.Tensor:
@@ -62,11 +64,27 @@ class ShardedHiveTable:
         dist.all_to_all_single(out, x, list(recv_counts), list(send_counts), group=self.group)
         return out
 
-    def apply(self, types, keys, vals) -> Tuple[torch.Tensor, torch.Tensor]:
+    @staticmethod
+    def _i32(x, dev) -> torch.Tensor:
+        """uint32 bit patterns as an int32 tensor on dev."""
+        t = torch.as_tensor(x)
+        if t.dtype != torch.int32:
+            t = t.to(torch.int64).to(torch.int32)
+        return t.to(dev)
+
+    @staticmethod
+    def _bytes(x: torch.Tensor) -> torch.Tensor:
+        """(n,) 4-byte tensor -> (n, 4) uint8 view of its bytes."""
+        return x.contiguous().view(torch.uint8).view(-1, 4)
+
+    def apply(self, types, keys, vals, local: Optional[LocalApply] = None) -> Tuple[torch.Tensor, torch.Tensor]:
+        """One batch of mixed ops (types as in HiveHashTable.apply) through the exchange; returns
+        (status u8, value i32) per op in submission order.  `local` replaces the shard's own
+        apply for this batch (insert() and find() pass the shard's bulk calls)."""
+        local = local or self._apply
         dev = self.device
-        types = torch.as_tensor(types).to(dev).to(torch.int64)
-        keys = torch.as_tensor(keys).to(dev).to(torch.int64)
-        vals = torch.as_tensor(vals).to(dev).to(torch.int64)
+        types = torch.as_tensor(types).to(dev).to(torch.uint8)
+        keys, vals = self._i32(keys, dev), self._i32(vals, dev)
         n = keys.numel()
         dest = owner_of(keys, self.world)
         order = torch.argsort(dest, stable=True)
@@ -74,27 +92,43 @@ class ShardedHiveTable:
         recv = torch.empty_like(send)
         dist.all_to_all_single(recv, send, group=self.group)
         send_l, recv_l = send.tolist(), recv.tolist()
-        # one record per op: [type, key, value]
-        rec = torch.stack([types[order], keys[order] & 0xFFFFFFFF, vals[order] & 0xFFFFFFFF], dim=1).contiguous()
-        got = self._a2a(rec, send_l, recv_l)
-        gt = got[:, 0].to(torch.uint8)
-        gk = got[:, 1].to(torch.int32)
-        gv = got[:, 2].to(torch.int32)
+        # one 9-byte record per op: key, value, type
+        rec = torch.cat([self._bytes(keys[order]), self._bytes(vals[order]), types[order].view(-1, 1)], dim=1)
+        got = self._a2a(rec.contiguous(), send_l, recv_l)
+        gk = got[:, 0:4].contiguous().view(torch.int32).view(-1)
+        gv = got[:, 4:8].contiguous().view(torch.int32).view(-1)
+        gt = got[:, 8].contiguous()
         if got.shape[0]:
-            st, ov = self._apply(gt, gk, gv)
-            res = torch.stack([st.to(torch.int64), ov.to(torch.int64) & 0xFFFFFFFF], dim=1).contiguous()
+            st, ov = local(gt, gk, gv)
+            st = st.to(dev).to(torch.uint8)
+            ov = ov.to(dev).to(torch.int32)
         else:
-            res = torch.empty((0, 2), dtype=torch.int64, device=dev)
+            st = torch.empty(0, dtype=torch.uint8, device=dev)
+            ov = torch.empty(0, dtype=torch.int32, device=dev)
+        # one 5-byte result per op: status, value
+        res = torch.cat([st.view(-1, 1), self._bytes(ov)], dim=1).contiguous()
         back = self._a2a(res, recv_l, send_l)
         status = torch.empty(n, dtype=torch.uint8, device=dev)
-        outv = torch.empty(n, dtype=torch.int64, device=dev)
-        status[order] = back[:, 0].to(torch.uint8)
-        outv[order] = back[:, 1]
-        return status, outv.to(torch.int32)
+        outv = torch.empty(n, dtype=torch.int32, device=dev)
+        status[order] = back[:, 0]
+        outv[order] = back[:, 1:5].contiguous().view(torch.int32).view(-1)
+        return status, outv
 
     def insert(self, keys, vals):
-        return self.apply(torch.zeros(len(keys), dtype=torch.uint8), keys, vals)[0]
+        """Bulk upsert; statuses as HiveHashTable.insert.  A HiveHashTable shard applies what it
+        receives with its bulk insert."""
+        t = self.local
+        bulk = None if t is None else (lambda _t, k, v: (t.insert(k, v), torch.zeros_like(k)))
+        return self.apply(torch.zeros(len(keys), dtype=torch.uint8), keys, vals, bulk)[0]
 
     def find(self, keys):
-        st, ov = self.apply(torch.ones(len(keys), dtype=torch.uint8), keys, torch.zeros(len(keys), dtype=torch.int32))
+        """Bulk lookup: (values, found).  A HiveHashTable shard answers with its bulk find."""
+        t = self.local
+
+        def bulk(_t, k, _v):
+            v, f = t.find(k)
+            return f, v
+
+        st, ov = self.apply(torch.ones(len(keys), dtype=torch.uint8), keys, torch.zeros(len(keys), dtype=torch.int32),
+                            None if t is None else bulk)
         return ov, st
