@@ -5,6 +5,7 @@ Outputs (git-ignored, shipped with the source tree):
   hivehashtable_b200/lib/libhive_compat.so   the reference's C++ API on top of the C ABI
   hivehashtable_b200/lib/libhive_workload.so seeded workload generator (host C++)
   hivehashtable_b200/lib/libhive_serve.so    the served request loop (host C++)
+  hivehashtable_b200/lib/libhive_shard.so    the sharded table's exchange kernels
 and, for bench.py only (build_probe), lib/libhive_probe.so: the random-access ceiling probes.
 
 Run as ``python -m hivehashtable_b200.build`` or through ``__graft_entry__.build()``.
@@ -106,8 +107,19 @@ def build_serve(force: bool = False) -> Path:
     return out
 
 
+def build_shard(force: bool = False) -> Path:
+    """The sharded table's exchange kernels (csrc/hive_shard.cu, include/hive_shard.h)."""
+    out = LIB / "libhive_shard.so"
+    src = CSRC / "hive_shard.cu"
+    if force or _stale(out, [src, INCLUDE / "hive_shard.h"]):
+        LIB.mkdir(exist_ok=True)
+        _run([_nvcc(), *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-fvisibility=hidden", f"-I{INCLUDE}", str(src), "-o", str(out), "-lcudart"])
+    return out
+
+
 def build_all(force: bool = False) -> list[Path]:
-    outs = [build_core(force), build_workload(force), build_serve(force)]
+    outs = [build_core(force), build_workload(force), build_serve(force), build_shard(force)]
     if (CSRC / "hive_compat.cpp").exists():
         outs.append(build_compat(force))
     return outs

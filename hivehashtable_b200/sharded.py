@@ -17,11 +17,36 @@ reference is single-GPU; this is the sharding it has no counterpart for.
 """
 from __future__ import annotations
 
+import ctypes
+from pathlib import Path
 from typing import Callable, Optional, Tuple
 
 import numpy as np
 import torch
 import torch.distributed as dist
+
+_SHARD_LIB = Path(__file__).resolve().parent / "lib" / "libhive_shard.so"
+_shard_lib = None
+
+
+def shard_library() -> ctypes.CDLL:
+    """libhive_shard.so: the exchange kernels (include/hive_shard.h).  Raises if not built."""
+    global _shard_lib
+    if _shard_lib is None:
+        if not _SHARD_LIB.exists():
+            raise ImportError(f"{_SHARD_LIB} is missing: build it with `python -m hivehashtable_b200.build`")
+        lib = ctypes.CDLL(str(_SHARD_LIB))
+        P, U64, U32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32
+        lib.hive_shard_blocks.restype = U64
+        lib.hive_shard_blocks.argtypes = [U64]
+        for name, args in (("hive_shard_count", [P, U64, U32, P, P]),
+                           ("hive_shard_scatter", [P, P, P, U64, U32, P, P, P, P, P, P]),
+                           ("hive_shard_gather", [P, U64, P, P, P, P, P])):
+            fn = getattr(lib, name)
+            fn.restype = ctypes.c_int
+            fn.argtypes = args
+        _shard_lib = lib
+    return _shard_lib
 
 
 def owner_of(keys_i32: torch.Tensor, world: int) -> torch.Tensor:
@@ -83,8 +108,10 @@ class ShardedHiveTable:
         apply for this batch (insert() and find() pass the shard's bulk calls)."""
         local = local or self._apply
         dev = self.device
-        types = torch.as_tensor(types).to(dev).to(torch.uint8)
-        keys, vals = self._i32(keys, dev), self._i32(vals, dev)
+        types = torch.as_tensor(types).to(dev).to(torch.uint8).contiguous()
+        keys, vals = self._i32(keys, dev).contiguous(), self._i32(vals, dev).contiguous()
+        if dev.type == "cuda":
+            return self._apply_device(types, keys, vals, local)
         n = keys.numel()
         dest = owner_of(keys, self.world)
         order = torch.argsort(dest, stable=True)
@@ -112,6 +139,47 @@ class ShardedHiveTable:
         outv = torch.empty(n, dtype=torch.int32, device=dev)
         status[order] = back[:, 0]
         outv[order] = back[:, 1:5].contiguous().view(torch.int32).view(-1)
+        return status, outv
+
+    def _apply_device(self, types, keys, vals, local) -> Tuple[torch.Tensor, torch.Tensor]:
+        """apply() with the batch on the GPU: the owner split by the native count/scatter kernels
+        (keys, values, types kept as separate arrays, so the exchange moves 9 bytes per op and the
+        shard reads them without unpacking), the results put back by the native gather."""
+        lib = shard_library()
+        dev = self.device
+        s = torch.cuda.current_stream(dev).cuda_stream
+        n, w = keys.numel(), self.world
+        nb = int(lib.hive_shard_blocks(n))
+        counts = torch.zeros(w * max(nb, 1), dtype=torch.int32, device=dev)
+        if n and lib.hive_shard_count(keys.data_ptr(), n, w, counts.data_ptr(), s):
+            raise RuntimeError("hive_shard_count failed")
+        c64 = counts.to(torch.int64)
+        starts = torch.cumsum(c64, 0) - c64
+        send = c64.view(w, -1).sum(1)
+        recv = torch.empty_like(send)
+        dist.all_to_all_single(recv, send, group=self.group)
+        out_k = torch.empty(n, dtype=torch.int32, device=dev)
+        out_v = torch.empty(n, dtype=torch.int32, device=dev)
+        out_t = torch.empty(n, dtype=torch.uint8, device=dev)
+        pos = torch.empty(n, dtype=torch.int64, device=dev)
+        if n and lib.hive_shard_scatter(keys.data_ptr(), vals.data_ptr(), types.data_ptr(), n, w, starts.data_ptr(),
+                                        out_k.data_ptr(), out_v.data_ptr(), out_t.data_ptr(), pos.data_ptr(), s):
+            raise RuntimeError("hive_shard_scatter failed")
+        send_l, recv_l = send.tolist(), recv.tolist()
+        gk, gv, gt = self._a2a(out_k, send_l, recv_l), self._a2a(out_v, send_l, recv_l), self._a2a(out_t, send_l, recv_l)
+        if gk.numel():
+            st, ov = local(gt, gk, gv)
+            st = st.to(dev).to(torch.uint8).contiguous()
+            ov = ov.to(dev).to(torch.int32).contiguous()
+        else:
+            st = torch.empty(0, dtype=torch.uint8, device=dev)
+            ov = torch.empty(0, dtype=torch.int32, device=dev)
+        back_st, back_v = self._a2a(st, recv_l, send_l), self._a2a(ov, recv_l, send_l)
+        status = torch.empty(n, dtype=torch.uint8, device=dev)
+        outv = torch.empty(n, dtype=torch.int32, device=dev)
+        if n and lib.hive_shard_gather(pos.data_ptr(), n, back_st.data_ptr(), back_v.data_ptr(), status.data_ptr(),
+                                       outv.data_ptr(), s):
+            raise RuntimeError("hive_shard_gather failed")
         return status, outv
 
     def insert(self, keys, vals):

@@ -1,4 +1,5 @@
-"""The C ABI library loads and exports every symbol include/hive_c.h declares (no GPU needed)."""
+"""The C ABI libraries load and export every symbol include/hive_c.h and include/hive_shard.h declare
+(no GPU needed)."""
 import ctypes
 import re
 import subprocess
@@ -64,3 +65,19 @@ def test_create_reports_missing_device():
     assert lib.hive_create(ctypes.byref(cfg), ctypes.byref(h)) == 7
     with pytest.raises(table.HiveError):
         table.HiveHashTable(1024)
+
+
+def test_shard_library_exports_its_header():
+    decl = _declared(ROOT / "include" / "hive_shard.h")
+    assert decl == ["hive_shard_blocks", "hive_shard_count", "hive_shard_gather", "hive_shard_scatter"]
+    exp = _exported(build.build_shard())
+    assert sorted(e for e in exp if e.startswith("hive_")) == decl
+    assert not [e for e in exp if not e.startswith("hive_")]
+    from hivehashtable_b200.sharded import shard_library
+
+    lib = shard_library()
+    assert lib.hive_shard_blocks(0) == 0 and lib.hive_shard_blocks(4096) == 1 and lib.hive_shard_blocks(4097) == 2
+    # argument checks run before any launch, so they need no device
+    assert lib.hive_shard_count(None, 10, 2, None, None) == 1
+    assert lib.hive_shard_scatter(None, None, None, 10, 2, None, None, None, None, None, None) == 1
+    assert lib.hive_shard_gather(None, 10, None, None, None, None, None) == 1

@@ -34,7 +34,7 @@ def _batches(seed, n_batches, size):
 
     pre, pool, _ = oracle.gen_keys(seed, 4 * size, n_batches * size * 2)
     rs = np.random.RandomState(seed)
-    live = list(pre)
+    live = sorted(set(pre.tolist()))
     out, pi = [], 0
     for _ in range(n_batches):
         new = pool[pi: pi + size // 2]
@@ -51,7 +51,7 @@ def _batches(seed, n_batches, size):
         keys, types, vals = keys[perm], types[perm], vals[perm]
         out.append((types, keys, vals))
         gone = set(keys[types == 2].tolist())
-        live = [k for k in live if k not in gone] + [int(k) for k in keys[types == 0]]
+        live = sorted((set(live) - gone) | set(keys[types == 0].tolist()))  # each key once
     return pre, out
 
 
@@ -137,3 +137,40 @@ def test_sharded_two_ranks_gloo_real_shards(cuda):
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
     sizes = dict(q.get() for _ in range(2))
     assert min(sizes.values()) > 0
+
+
+@pytest.mark.parametrize("world,n", [(3, 100_003), (8, 1 << 20), (1, 5000)])
+def test_exchange_kernels_split_by_owner(cuda, world, n):
+    """hive_shard_count / scatter / gather: every op lands in its owner's range (owner as
+    sharded.owner_of computes it), pos is a permutation, and gather inverts scatter."""
+    import oracle
+    from hivehashtable_b200.sharded import owner_of, shard_library
+
+    lib = shard_library()
+    keys, _, _ = oracle.gen_keys(51, n, 0)
+    kd = torch.from_numpy(keys.view(np.int32)).to(cuda)
+    vd = torch.arange(n, dtype=torch.int32, device=cuda)
+    td = (torch.arange(n, device=cuda) % 4).to(torch.uint8)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    nb = int(lib.hive_shard_blocks(n))
+    counts = torch.zeros(world * nb, dtype=torch.int32, device=cuda)
+    assert lib.hive_shard_count(kd.data_ptr(), n, world, counts.data_ptr(), s) == 0
+    c64 = counts.to(torch.int64)
+    starts = torch.cumsum(c64, 0) - c64
+    ok, ov, ot = (torch.empty(n, dtype=d, device=cuda) for d in (torch.int32, torch.int32, torch.uint8))
+    pos = torch.empty(n, dtype=torch.int64, device=cuda)
+    assert lib.hive_shard_scatter(kd.data_ptr(), vd.data_ptr(), td.data_ptr(), n, world, starts.data_ptr(),
+                                  ok.data_ptr(), ov.data_ptr(), ot.data_ptr(), pos.data_ptr(), s) == 0
+    own = owner_of(kd, world)
+    per_rank = torch.bincount(own, minlength=world)
+    assert torch.equal(c64.view(world, -1).sum(1), per_rank)
+    p = pos.cpu().numpy()
+    assert np.array_equal(np.sort(p), np.arange(n))
+    bounds = np.concatenate([[0], np.cumsum(per_rank.cpu().numpy())])
+    rank_of_place = np.searchsorted(bounds, p, side="right") - 1
+    assert np.array_equal(rank_of_place, own.cpu().numpy())
+    assert torch.equal(ok[pos], kd) and torch.equal(ov[pos], vd) and torch.equal(ot[pos], td)
+    st = torch.empty(n, dtype=torch.uint8, device=cuda)
+    back = torch.empty(n, dtype=torch.int32, device=cuda)
+    assert lib.hive_shard_gather(pos.data_ptr(), n, ot.data_ptr(), ov.data_ptr(), st.data_ptr(), back.data_ptr(), s) == 0
+    assert torch.equal(st, td) and torch.equal(back, vd)
