@@ -9,7 +9,10 @@
 //              by key: a group whose first request is a lookup needs the key's value before the
 //              batch (one device lookup); a group with writes needs one device upsert of its last
 //              written value.  Lookups after a write in the same batch are answered from that
-//              write, so every result equals the one a one-at-a-time replay in arrival order gives
+//              write, so every result equals the one a one-at-a-time replay in arrival order gives.
+//              Batches of 4096 requests or more are split by key over host_threads workers (all
+//              requests of a key go to one worker, in arrival order), each with its own map; the
+//              answers are split the same way
 //   launch     pinned-host -> device copies on the slot's copy stream; the lookups, then the
 //              upserts, on the single compute stream (batches therefore reach the table in
 //              arrival order); the results back on the copy stream
@@ -33,10 +36,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
+#include <thread>
 #include <vector>
 
 #include "hive_serve.h"
@@ -44,6 +50,66 @@
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+// Host workers for batch formation and answering: run(f) calls f(w) on every worker w (the
+// calling thread is worker 0) and returns when all have finished.  Idle workers spin on a
+// generation counter (yielding now and then), since a batch is formed every few microseconds.
+class WorkerPool {
+  public:
+    explicit WorkerPool(int n) : n_(n) {
+        for (int w = 1; w < n; ++w) threads_.emplace_back([this, w] { loop(w); });
+    }
+    ~WorkerPool() {
+        stop_.store(true, std::memory_order_release);
+        for (auto& t : threads_) t.join();
+    }
+    int size() const { return n_; }
+    void run(const std::function<void(int)>& f) {
+        if (n_ == 1) {
+            f(0);
+            return;
+        }
+        job_ = &f;
+        left_.store(n_ - 1, std::memory_order_relaxed);
+        gen_.fetch_add(1, std::memory_order_release);
+        f(0);
+        for (int spin = 0; left_.load(std::memory_order_acquire) != 0; ++spin)
+            if ((spin & 255) == 255) std::this_thread::yield();
+    }
+
+  private:
+    void loop(int w) {
+        uint64_t seen = 0;
+        for (;;) {
+            uint64_t g;
+            for (int spin = 0; (g = gen_.load(std::memory_order_acquire)) == seen; ++spin) {
+                if (stop_.load(std::memory_order_acquire)) return;
+                if ((spin & 255) == 255) std::this_thread::yield();
+            }
+            seen = g;
+            (*job_)(w);
+            left_.fetch_sub(1, std::memory_order_acq_rel);
+        }
+    }
+    int n_;
+    std::vector<std::thread> threads_;
+    std::atomic<uint64_t> gen_{0};
+    std::atomic<int> left_{0};
+    std::atomic<bool> stop_{false};
+    const std::function<void(int)>* job_ = nullptr;
+};
+
+// The worker that coalesces key k: requests of one key all go to one worker, which sees them in
+// arrival order.
+inline int part_of(uint32_t k, int parts) {
+    uint32_t h = k ^ 0x6A09E667u;
+    h ^= h >> 15;
+    h *= 0x2c1b3c6du;
+    h ^= h >> 12;
+    h *= 0x297a2d39u;
+    h ^= h >> 15;
+    return (int)(((uint64_t)h * (uint64_t)parts) >> 32);
+}
 
 // Key -> group index of one batch: open addressing with linear probing over a power-of-two table
 // at least twice the batch size.  A slot belongs to the current batch iff its stamp equals the
@@ -94,6 +160,18 @@ class GroupMap {
     uint32_t mask_ = 0, gen_ = 0;
 };
 
+// One worker's share of a batch: its requests (offsets in the batch, ascending) and its key
+// groups; positions in the lookup / upsert lists are local and start at f_off / u_off.
+struct Part {
+    std::vector<uint32_t> reqs;
+    std::vector<int32_t> find_of;    // group -> local lookup position, or -1
+    std::vector<int32_t> upsert_of;  // group -> local upsert position, or -1
+    std::vector<uint32_t> fkeys, ukeys, uvals;
+    uint32_t f_off = 0, u_off = 0;
+    uint64_t new_writes = 0;
+    uint64_t placed_new = 0;
+};
+
 struct Slot {
     cudaStream_t copy = nullptr;
     cudaEvent_t staged = nullptr, done = nullptr;
@@ -105,10 +183,8 @@ struct Slot {
     uint8_t *d_ftypes = nullptr, *d_utypes = nullptr, *d_found = nullptr, *d_ust = nullptr;
     // the batch: requests [first, first + count) in arrival order
     uint64_t first = 0, count = 0;
-    std::vector<int32_t> group;       // group of each request
-    std::vector<int32_t> lastw;       // group -> latest write answered so far (finish), or -1
-    std::vector<int32_t> find_of;     // group -> position in the lookup list or -1
-    std::vector<int32_t> upsert_of;   // group -> position in the upsert list or -1
+    std::vector<int32_t> group;       // each request's group within its worker's part
+    std::vector<Part> parts;          // one per worker
     uint32_t nf = 0, nu = 0;
     uint64_t new_writes = 0;          // distinct written keys of the batch (possible new keys)
     bool busy = false;
@@ -179,7 +255,8 @@ int hive_serve_run(
     hive_serve_stats* stats) {
     if (!t || !cfg || !types || !keys || !vals || !arrival_s || !out_vals || !out_status || !done_s)
         return HIVE_ERR_INVALID_ARG;
-    if (cfg->depth < 1 || cfg->depth > 64 || cfg->max_batch < 1) return HIVE_ERR_INVALID_ARG;
+    if (cfg->depth < 1 || cfg->depth > 64 || cfg->max_batch < 1 || cfg->host_threads > 64 || cfg->reserved != 0)
+        return HIVE_ERR_INVALID_ARG;
     if (!(cfg->grow_start >= 0.0) || (cfg->grow_start > 0.0 && !(cfg->grow_start < cfg->max_load)))
         return HIVE_ERR_INVALID_ARG;
     hive_serve_stats st{};
@@ -196,43 +273,65 @@ int hive_serve_run(
     uint64_t grow_target = 0, grow_step = 0;  // incremental growth: target buckets, buckets per step
     uint64_t grow_refused_at = 0;             // bucket count at which growth found no memory
 
-    GroupMap gid(cap);
-    std::vector<uint32_t> g_key;    // group -> key
-    std::vector<uint32_t> g_lastw;  // group -> index (within the batch) of its last write, or ~0
+    // host workers: partitions of a batch by key (part_of), each coalesced by its own worker
+    int nworkers = (int)cfg->host_threads;
+    if (nworkers <= 0) nworkers = (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency() / 2));
+    nworkers = std::min(nworkers, 64);
+    WorkerPool pool(nworkers);
+    std::vector<GroupMap> gmaps;
+    for (int w = 0; w < nworkers; ++w) gmaps.emplace_back(cap);
+    std::vector<std::vector<uint32_t>> w_lastw(nworkers), w_key(nworkers);  // per-worker scratch
+    std::vector<std::vector<int32_t>> w_answered(nworkers);
+    for (auto& s : slots) s.parts.resize(nworkers);
+    // a batch smaller than this is formed by the calling thread alone (no hand-off)
+    constexpr uint64_t kParallelMin = 4096;
     // Requests are admitted in arrival order, so the pending ones are always [pend, next).
     uint64_t pend = 0, next = 0, finished = 0;
     size_t head = 0;                // ring position of the oldest in-flight slot
     size_t in_flight = 0;
     const auto t0 = Clock::now();
     auto now_s = [&] { return std::chrono::duration<double>(Clock::now() - t0).count(); };
+    auto run_parts = [&](int nparts, const std::function<void(int)>& f) {
+        if (nparts == 1) f(0);
+        else pool.run(f);
+    };
 
     auto finish = [&](Slot& s) {
-        // answers of the batch, in request order
-        std::vector<int32_t>& lastw = s.lastw;
-        lastw.assign(s.find_of.size(), -1);
-        for (uint64_t j = 0; j < s.count; ++j) {
-            const uint64_t r = s.first + j;
-            const int32_t g = s.group[j];
-            if (types[r] == HIVE_OP_LOOKUP) {
-                if (lastw[g] >= 0) {
-                    out_vals[r] = vals[s.first + lastw[g]];
-                    out_status[r] = 1;
+        // answers of the batch: each worker answers its own requests in arrival order; a lookup
+        // after a write of its key in the batch is answered from that write
+        const int nparts = s.count >= kParallelMin ? nworkers : 1;
+        run_parts(nparts, [&](int w) {
+            Part& P = s.parts[w];
+            std::vector<int32_t>& lastw = w_answered[w];
+            lastw.assign(P.find_of.size(), -1);
+            for (const uint32_t j : P.reqs) {
+                const uint64_t r = s.first + j;
+                const int32_t g = s.group[j];
+                if (types[r] == HIVE_OP_LOOKUP) {
+                    if (lastw[g] >= 0) {
+                        out_vals[r] = vals[s.first + lastw[g]];
+                        out_status[r] = 1;
+                    } else {
+                        const uint32_t f = P.f_off + (uint32_t)P.find_of[g];
+                        out_status[r] = s.h_found[f];
+                        out_vals[r] = s.h_found[f] ? s.h_fvals[f] : 0u;
+                    }
                 } else {
-                    const int32_t f = s.find_of[g];
-                    out_status[r] = s.h_found[f];
-                    out_vals[r] = s.h_found[f] ? s.h_fvals[f] : 0u;
+                    lastw[g] = (int32_t)j;
+                    const int32_t u = P.upsert_of[g];
+                    const uint8_t us = u >= 0 ? s.h_ust[P.u_off + u] : 0;
+                    out_status[r] = (us != HIVE_ST_FAIL && us != HIVE_ST_ERROR) ? 1 : 0;
+                    out_vals[r] = 0;
                 }
-            } else {
-                lastw[g] = (int32_t)j;
-                const int32_t u = s.upsert_of[g];
-                const uint8_t us = u >= 0 ? s.h_ust[u] : 0;
-                out_status[r] = (us != HIVE_ST_FAIL && us != HIVE_ST_ERROR) ? 1 : 0;
-                out_vals[r] = 0;
             }
-        }
-        uint64_t placed_new = 0;
-        for (uint32_t u = 0; u < s.nu; ++u) placed_new += s.h_ust[u] == HIVE_ST_INSERTED || s.h_ust[u] == HIVE_ST_STASHED;
-        live_done += placed_new;
+            uint64_t placed = 0;
+            for (uint32_t u = 0; u < (uint32_t)P.ukeys.size(); ++u) {
+                const uint8_t us = s.h_ust[P.u_off + u];
+                placed += us == HIVE_ST_INSERTED || us == HIVE_ST_STASHED;
+            }
+            P.placed_new = placed;
+        });
+        for (int w = 0; w < nparts; ++w) live_done += s.parts[w].placed_new;
         pending_new -= s.new_writes;
         const double td = now_s();
         std::fill(done_s + s.first, done_s + s.first + s.count, td);
@@ -281,44 +380,79 @@ int hive_serve_run(
         s.first = pend;
         s.count = take;
         pend += take;
-        gid.next_batch();
+        const int nparts = take >= kParallelMin ? nworkers : 1;
         s.group.resize(take);
-        s.find_of.clear();
-        s.upsert_of.clear();
-        g_lastw.clear();
-        g_key.clear();
+        run_parts(nparts, [&](int w) {
+            // coalesce this worker's keys: a group whose first request is a lookup needs one device
+            // lookup; a group with writes needs one device upsert of its last written value
+            Part& P = s.parts[w];
+            GroupMap& gm = gmaps[w];
+            std::vector<uint32_t>& g_lastw = w_lastw[w];
+            std::vector<uint32_t>& g_key = w_key[w];
+            gm.next_batch();
+            P.reqs.clear();
+            P.find_of.clear();
+            P.upsert_of.clear();
+            P.fkeys.clear();
+            P.ukeys.clear();
+            P.uvals.clear();
+            g_lastw.clear();
+            g_key.clear();
+            uint64_t nw = 0;
+            for (uint64_t j = 0; j < take; ++j) {
+                const uint64_t r = s.first + j;
+                const uint32_t k = keys[r];
+                if (nparts > 1 && part_of(k, nparts) != w) continue;
+                P.reqs.push_back((uint32_t)j);
+                bool added;
+                const int32_t g = gm.find_or_add(k, (int32_t)P.find_of.size(), &added);
+                if (added) {
+                    P.find_of.push_back(types[r] == HIVE_OP_LOOKUP ? -2 : -1);  // -2: needs a lookup
+                    P.upsert_of.push_back(-1);
+                    g_lastw.push_back(0xFFFFFFFFu);
+                    g_key.push_back(k);
+                }
+                s.group[j] = g;
+                if (types[r] != HIVE_OP_LOOKUP) {
+                    if (g_lastw[g] == 0xFFFFFFFFu) ++nw;
+                    g_lastw[g] = (uint32_t)j;
+                }
+            }
+            for (size_t g = 0; g < P.find_of.size(); ++g) {
+                if (P.find_of[g] == -2) {
+                    P.find_of[g] = (int32_t)P.fkeys.size();
+                    P.fkeys.push_back(g_key[g]);
+                } else {
+                    P.find_of[g] = -1;
+                }
+                if (g_lastw[g] != 0xFFFFFFFFu) {
+                    const uint64_t r = s.first + g_lastw[g];
+                    P.upsert_of[g] = (int32_t)P.ukeys.size();
+                    P.ukeys.push_back(keys[r]);
+                    P.uvals.push_back(vals[r]);
+                }
+            }
+            P.new_writes = nw;
+        });
+        // the workers' lists, one after another, in the slot's pinned staging
         uint64_t new_writes = 0;
-        for (uint64_t j = 0; j < take; ++j) {
-            const uint64_t r = s.first + j;
-            bool added;
-            const int32_t g = gid.find_or_add(keys[r], (int32_t)s.find_of.size(), &added);
-            if (added) {
-                s.find_of.push_back(types[r] == HIVE_OP_LOOKUP ? -2 : -1);  // -2: needs a lookup
-                s.upsert_of.push_back(-1);
-                g_lastw.push_back(0xFFFFFFFFu);
-                g_key.push_back(keys[r]);
-            }
-            s.group[j] = g;
-            if (types[r] != HIVE_OP_LOOKUP) {
-                if (g_lastw[g] == 0xFFFFFFFFu) ++new_writes;
-                g_lastw[g] = (uint32_t)j;
-            }
-        }
         s.nf = s.nu = 0;
-        for (size_t g = 0; g < s.find_of.size(); ++g) {
-            if (s.find_of[g] == -2) {
-                s.h_fkeys[s.nf] = g_key[g];
-                s.find_of[g] = (int32_t)s.nf++;
-            } else {
-                s.find_of[g] = -1;
-            }
-            if (g_lastw[g] != 0xFFFFFFFFu) {
-                const uint64_t r = s.first + g_lastw[g];
-                s.h_ukeys[s.nu] = keys[r];
-                s.h_uvals[s.nu] = vals[r];
-                s.upsert_of[g] = (int32_t)s.nu++;
-            }
+        for (int w = 0; w < nparts; ++w) {
+            Part& P = s.parts[w];
+            P.f_off = s.nf;
+            P.u_off = s.nu;
+            s.nf += (uint32_t)P.fkeys.size();
+            s.nu += (uint32_t)P.ukeys.size();
+            new_writes += P.new_writes;
         }
+        run_parts(nparts, [&](int w) {
+            const Part& P = s.parts[w];
+            if (!P.fkeys.empty()) std::memcpy(s.h_fkeys + P.f_off, P.fkeys.data(), P.fkeys.size() * 4);
+            if (!P.ukeys.empty()) {
+                std::memcpy(s.h_ukeys + P.u_off, P.ukeys.data(), P.ukeys.size() * 4);
+                std::memcpy(s.h_uvals + P.u_off, P.uvals.data(), P.uvals.size() * 4);
+            }
+        });
         // growth: keep the load factor under max_load counting every write in flight as a new key
         if (cfg->max_load > 0.0 && new_writes) {
             hive_get_info(t, &info);
