@@ -297,6 +297,7 @@ int hive_serve_run(
     };
 
     auto finish = [&](Slot& s) {
+        const double ta = now_s();
         // answers of the batch: each worker answers its own requests in arrival order; a lookup
         // after a write of its key in the batch is answered from that write
         const int nparts = s.count >= kParallelMin ? nworkers : 1;
@@ -337,6 +338,7 @@ int hive_serve_run(
         std::fill(done_s + s.first, done_s + s.first + s.count, td);
         finished += s.count;
         s.busy = false;
+        st.answer_s += now_s() - ta;
     };
 
     auto drain = [&] {
@@ -372,9 +374,11 @@ int hive_serve_run(
                 while (now_s() < arrival_s[next]) {
                 }
             }
+            st.idle_s += now_s() - tn;
             continue;
         }
         // form a batch
+        const double tf = now_s();
         Slot& s = slots[tail];
         const uint64_t take = std::min<uint64_t>(next - pend, cap);
         s.first = pend;
@@ -513,6 +517,8 @@ int hive_serve_run(
         pending_new += new_writes;
         s.new_writes = new_writes;
         // launch
+        const double tl = now_s();
+        st.form_s += tl - tf;
         if (s.nf && cudaMemcpyAsync(s.d_fkeys, s.h_fkeys, (size_t)s.nf * 4, cudaMemcpyHostToDevice, s.copy)) rc = HIVE_ERR_CUDA;
         if (s.nu && (cudaMemcpyAsync(s.d_ukeys, s.h_ukeys, (size_t)s.nu * 4, cudaMemcpyHostToDevice, s.copy) ||
                      cudaMemcpyAsync(s.d_uvals, s.h_uvals, (size_t)s.nu * 4, cudaMemcpyHostToDevice, s.copy)))
@@ -536,6 +542,7 @@ int hive_serve_run(
         if (s.nu && cudaMemcpyAsync(s.h_ust, s.d_ust, s.nu, cudaMemcpyDeviceToHost, s.copy)) rc = HIVE_ERR_CUDA;
         cudaEventRecord(s.done, s.copy);
         st.batches++;
+        st.launch_s += now_s() - tl;
         st.device_lookups += s.nf;
         st.device_upserts += s.nu;
         s.busy = true;

@@ -31,7 +31,9 @@ class ServeConfig(ctypes.Structure):
 class ServeStats(ctypes.Structure):
     _fields_ = [("batches", ctypes.c_uint64), ("device_lookups", ctypes.c_uint64),
                 ("device_upserts", ctypes.c_uint64), ("resizes", ctypes.c_uint64), ("refused", ctypes.c_uint64),
-                ("wall_s", ctypes.c_double), ("grow_steps", ctypes.c_uint64), ("drains", ctypes.c_uint64)]
+                ("wall_s", ctypes.c_double), ("grow_steps", ctypes.c_uint64), ("drains", ctypes.c_uint64),
+                ("form_s", ctypes.c_double), ("launch_s", ctypes.c_double), ("answer_s", ctypes.c_double),
+                ("idle_s", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -51,6 +51,10 @@ typedef struct hive_serve_stats {
     double wall_s;           /* call start to last completion                                */
     uint64_t grow_steps;     /* bounded split steps run between batches by incremental growth */
     uint64_t drains;         /* growths that had to drain the pipeline first                 */
+    double form_s;           /* host time forming batches (admission and coalescing)         */
+    double launch_s;         /* host time queueing copies and table calls                    */
+    double answer_s;         /* host time answering finished batches                         */
+    double idle_s;           /* host time with nothing to do: waiting for arrivals or batches */
 } hive_serve_stats;
 
 int hive_serve_run(hive_table* t, const hive_serve_config* cfg, const uint8_t* types, const uint32_t* keys,
