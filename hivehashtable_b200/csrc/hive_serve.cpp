@@ -10,9 +10,8 @@
 //              batch (one device lookup); a group with writes needs one device upsert of its last
 //              written value.  Lookups after a write in the same batch are answered from that
 //              write, so every result equals the one a one-at-a-time replay in arrival order gives.
-//              Batches of 4096 requests or more are split by key over host_threads workers (all
-//              requests of a key go to one worker, in arrival order), each with its own map; the
-//              answers are split the same way
+//              Each request's answer source (the write that answers it, or its key group) is fixed
+//              while the batch is formed, so answering is one pass in request order
 //   launch     pinned-host -> device copies on the slot's copy stream; the lookups, then the
 //              upserts, on the single compute stream (batches therefore reach the table in
 //              arrival order); the results back on the copy stream
@@ -36,13 +35,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
-#include <functional>
-#include <thread>
 #include <vector>
 
 #include "hive_serve.h"
@@ -51,82 +47,21 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-// Host workers for batch formation and answering: run(f) calls f(w) on every worker w (the
-// calling thread is worker 0) and returns when all have finished.  Idle workers spin on a
-// generation counter (yielding now and then), since a batch is formed every few microseconds.
-class WorkerPool {
-  public:
-    explicit WorkerPool(int n) : n_(n) {
-        for (int w = 1; w < n; ++w) threads_.emplace_back([this, w] { loop(w); });
-    }
-    ~WorkerPool() {
-        stop_.store(true, std::memory_order_release);
-        for (auto& t : threads_) t.join();
-    }
-    int size() const { return n_; }
-    void run(const std::function<void(int)>& f) {
-        if (n_ == 1) {
-            f(0);
-            return;
-        }
-        job_ = &f;
-        left_.store(n_ - 1, std::memory_order_relaxed);
-        gen_.fetch_add(1, std::memory_order_release);
-        f(0);
-        for (int spin = 0; left_.load(std::memory_order_acquire) != 0; ++spin)
-            if ((spin & 255) == 255) std::this_thread::yield();
-    }
-
-  private:
-    void loop(int w) {
-        uint64_t seen = 0;
-        for (;;) {
-            uint64_t g;
-            for (int spin = 0; (g = gen_.load(std::memory_order_acquire)) == seen; ++spin) {
-                if (stop_.load(std::memory_order_acquire)) return;
-                if ((spin & 255) == 255) std::this_thread::yield();
-            }
-            seen = g;
-            (*job_)(w);
-            left_.fetch_sub(1, std::memory_order_acq_rel);
-        }
-    }
-    int n_;
-    std::vector<std::thread> threads_;
-    std::atomic<uint64_t> gen_{0};
-    std::atomic<int> left_{0};
-    std::atomic<bool> stop_{false};
-    const std::function<void(int)>* job_ = nullptr;
-};
-
-// The worker that coalesces key k: requests of one key all go to one worker, which sees them in
-// arrival order.
-inline int part_of(uint32_t k, int parts) {
-    uint32_t h = k ^ 0x6A09E667u;
-    h ^= h >> 15;
-    h *= 0x2c1b3c6du;
-    h ^= h >> 12;
-    h *= 0x297a2d39u;
-    h ^= h >> 15;
-    return (int)(((uint64_t)h * (uint64_t)parts) >> 32);
-}
-
 // Key -> group index of one batch: open addressing with linear probing over a power-of-two table
-// at least twice the batch size.  A slot belongs to the current batch iff its stamp equals the
-// batch's generation, so starting a batch costs one increment instead of a clear.
+// at least twice the batch size, one 16-byte entry per slot (key, group, batch stamp) so a probe
+// touches one cache line.  An entry belongs to the current batch iff its stamp equals the batch's
+// generation, so starting a batch costs one increment instead of a clear.
 class GroupMap {
   public:
     explicit GroupMap(uint32_t max_keys) {
         uint32_t sz = 16;
         while (sz < 2u * max_keys) sz <<= 1;
         mask_ = sz - 1;
-        keys_.resize(sz);
-        vals_.resize(sz);
-        stamp_.assign(sz, 0u);
+        e_.assign(sz, Entry{0u, 0, 0u, 0u});
     }
     void next_batch() {
         if (++gen_ == 0) {  // stamps wrapped: clear once every 2^32 batches
-            std::fill(stamp_.begin(), stamp_.end(), 0u);
+            for (auto& x : e_) x.stamp = 0u;
             gen_ = 1;
         }
     }
@@ -139,37 +74,28 @@ class GroupMap {
         h *= 0xc2b2ae35u;
         h ^= h >> 16;
         for (uint32_t i = h & mask_;; i = (i + 1) & mask_) {
-            if (stamp_[i] != gen_) {
-                stamp_[i] = gen_;
-                keys_[i] = k;
-                vals_[i] = fresh;
+            Entry& x = e_[i];
+            if (x.stamp != gen_) {
+                x = Entry{k, fresh, gen_, 0u};
                 *added = true;
                 return fresh;
             }
-            if (keys_[i] == k) {
+            if (x.key == k) {
                 *added = false;
-                return vals_[i];
+                return x.group;
             }
         }
     }
 
   private:
-    std::vector<uint32_t> keys_;
-    std::vector<int32_t> vals_;
-    std::vector<uint32_t> stamp_;
+    struct Entry {
+        uint32_t key;
+        int32_t group;
+        uint32_t stamp;
+        uint32_t pad;
+    };
+    std::vector<Entry> e_;
     uint32_t mask_ = 0, gen_ = 0;
-};
-
-// One worker's share of a batch: its requests (offsets in the batch, ascending) and its key
-// groups; positions in the lookup / upsert lists are local and start at f_off / u_off.
-struct Part {
-    std::vector<uint32_t> reqs;
-    std::vector<int32_t> find_of;    // group -> local lookup position, or -1
-    std::vector<int32_t> upsert_of;  // group -> local upsert position, or -1
-    std::vector<uint32_t> fkeys, ukeys, uvals;
-    uint32_t f_off = 0, u_off = 0;
-    uint64_t new_writes = 0;
-    uint64_t placed_new = 0;
 };
 
 struct Slot {
@@ -183,8 +109,11 @@ struct Slot {
     uint8_t *d_ftypes = nullptr, *d_utypes = nullptr, *d_found = nullptr, *d_ust = nullptr;
     // the batch: requests [first, first + count) in arrival order
     uint64_t first = 0, count = 0;
-    std::vector<int32_t> group;       // each request's group within its worker's part
-    std::vector<Part> parts;          // one per worker
+    // how each request is answered: >= 0, a lookup answered by that earlier write of the batch
+    // (offset in the batch); < 0, -(g + 1) for key group g (a lookup: the group's device lookup;
+    // a write: the group's device upsert)
+    std::vector<int32_t> ans;
+    std::vector<int32_t> fpos, upos;  // group -> position in the lookup / upsert list, or -1
     uint32_t nf = 0, nu = 0;
     uint64_t new_writes = 0;          // distinct written keys of the batch (possible new keys)
     bool busy = false;
@@ -255,8 +184,7 @@ int hive_serve_run(
     hive_serve_stats* stats) {
     if (!t || !cfg || !types || !keys || !vals || !arrival_s || !out_vals || !out_status || !done_s)
         return HIVE_ERR_INVALID_ARG;
-    if (cfg->depth < 1 || cfg->depth > 64 || cfg->max_batch < 1 || cfg->host_threads > 64 || cfg->reserved != 0)
-        return HIVE_ERR_INVALID_ARG;
+    if (cfg->depth < 1 || cfg->depth > 64 || cfg->max_batch < 1) return HIVE_ERR_INVALID_ARG;
     if (!(cfg->grow_start >= 0.0) || (cfg->grow_start > 0.0 && !(cfg->grow_start < cfg->max_load)))
         return HIVE_ERR_INVALID_ARG;
     hive_serve_stats st{};
@@ -273,66 +201,41 @@ int hive_serve_run(
     uint64_t grow_target = 0, grow_step = 0;  // incremental growth: target buckets, buckets per step
     uint64_t grow_refused_at = 0;             // bucket count at which growth found no memory
 
-    // host workers: partitions of a batch by key (part_of), each coalesced by its own worker
-    int nworkers = (int)cfg->host_threads;
-    if (nworkers <= 0) nworkers = (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency() / 2));
-    nworkers = std::min(nworkers, 64);
-    WorkerPool pool(nworkers);
-    std::vector<GroupMap> gmaps;
-    for (int w = 0; w < nworkers; ++w) gmaps.emplace_back(cap);
-    std::vector<std::vector<uint32_t>> w_lastw(nworkers), w_key(nworkers);  // per-worker scratch
-    std::vector<std::vector<int32_t>> w_answered(nworkers);
-    for (auto& s : slots) s.parts.resize(nworkers);
-    // a batch smaller than this is formed by the calling thread alone (no hand-off)
-    constexpr uint64_t kParallelMin = 4096;
+    GroupMap gid(cap);
+    std::vector<uint32_t> g_key;    // group -> key
+    std::vector<int32_t> g_lastw;   // group -> offset of its latest write so far, or -1
+    std::vector<uint8_t> g_look;    // group -> its first request is a lookup
     // Requests are admitted in arrival order, so the pending ones are always [pend, next).
     uint64_t pend = 0, next = 0, finished = 0;
     size_t head = 0;                // ring position of the oldest in-flight slot
     size_t in_flight = 0;
     const auto t0 = Clock::now();
     auto now_s = [&] { return std::chrono::duration<double>(Clock::now() - t0).count(); };
-    auto run_parts = [&](int nparts, const std::function<void(int)>& f) {
-        if (nparts == 1) f(0);
-        else pool.run(f);
-    };
 
     auto finish = [&](Slot& s) {
         const double ta = now_s();
-        // answers of the batch: each worker answers its own requests in arrival order; a lookup
-        // after a write of its key in the batch is answered from that write
-        const int nparts = s.count >= kParallelMin ? nworkers : 1;
-        run_parts(nparts, [&](int w) {
-            Part& P = s.parts[w];
-            std::vector<int32_t>& lastw = w_answered[w];
-            lastw.assign(P.find_of.size(), -1);
-            for (const uint32_t j : P.reqs) {
-                const uint64_t r = s.first + j;
-                const int32_t g = s.group[j];
-                if (types[r] == HIVE_OP_LOOKUP) {
-                    if (lastw[g] >= 0) {
-                        out_vals[r] = vals[s.first + lastw[g]];
-                        out_status[r] = 1;
-                    } else {
-                        const uint32_t f = P.f_off + (uint32_t)P.find_of[g];
-                        out_status[r] = s.h_found[f];
-                        out_vals[r] = s.h_found[f] ? s.h_fvals[f] : 0u;
-                    }
+        // answers of the batch, in request order, from the sources fixed when it was formed
+        for (uint64_t j = 0; j < s.count; ++j) {
+            const uint64_t r = s.first + j;
+            const int32_t a = s.ans[j];
+            if (types[r] == HIVE_OP_LOOKUP) {
+                if (a >= 0) {
+                    out_vals[r] = vals[s.first + a];
+                    out_status[r] = 1;
                 } else {
-                    lastw[g] = (int32_t)j;
-                    const int32_t u = P.upsert_of[g];
-                    const uint8_t us = u >= 0 ? s.h_ust[P.u_off + u] : 0;
-                    out_status[r] = (us != HIVE_ST_FAIL && us != HIVE_ST_ERROR) ? 1 : 0;
-                    out_vals[r] = 0;
+                    const int32_t f = s.fpos[-a - 1];
+                    out_status[r] = s.h_found[f];
+                    out_vals[r] = s.h_found[f] ? s.h_fvals[f] : 0u;
                 }
+            } else {
+                const uint8_t us = s.h_ust[s.upos[-a - 1]];
+                out_status[r] = (us != HIVE_ST_FAIL && us != HIVE_ST_ERROR) ? 1 : 0;
+                out_vals[r] = 0;
             }
-            uint64_t placed = 0;
-            for (uint32_t u = 0; u < (uint32_t)P.ukeys.size(); ++u) {
-                const uint8_t us = s.h_ust[P.u_off + u];
-                placed += us == HIVE_ST_INSERTED || us == HIVE_ST_STASHED;
-            }
-            P.placed_new = placed;
-        });
-        for (int w = 0; w < nparts; ++w) live_done += s.parts[w].placed_new;
+        }
+        uint64_t placed_new = 0;
+        for (uint32_t u = 0; u < s.nu; ++u) placed_new += s.h_ust[u] == HIVE_ST_INSERTED || s.h_ust[u] == HIVE_ST_STASHED;
+        live_done += placed_new;
         pending_new -= s.new_writes;
         const double td = now_s();
         std::fill(done_s + s.first, done_s + s.first + s.count, td);
@@ -384,79 +287,52 @@ int hive_serve_run(
         s.first = pend;
         s.count = take;
         pend += take;
-        const int nparts = take >= kParallelMin ? nworkers : 1;
-        s.group.resize(take);
-        run_parts(nparts, [&](int w) {
-            // coalesce this worker's keys: a group whose first request is a lookup needs one device
-            // lookup; a group with writes needs one device upsert of its last written value
-            Part& P = s.parts[w];
-            GroupMap& gm = gmaps[w];
-            std::vector<uint32_t>& g_lastw = w_lastw[w];
-            std::vector<uint32_t>& g_key = w_key[w];
-            gm.next_batch();
-            P.reqs.clear();
-            P.find_of.clear();
-            P.upsert_of.clear();
-            P.fkeys.clear();
-            P.ukeys.clear();
-            P.uvals.clear();
-            g_lastw.clear();
-            g_key.clear();
-            uint64_t nw = 0;
-            for (uint64_t j = 0; j < take; ++j) {
-                const uint64_t r = s.first + j;
-                const uint32_t k = keys[r];
-                if (nparts > 1 && part_of(k, nparts) != w) continue;
-                P.reqs.push_back((uint32_t)j);
-                bool added;
-                const int32_t g = gm.find_or_add(k, (int32_t)P.find_of.size(), &added);
-                if (added) {
-                    P.find_of.push_back(types[r] == HIVE_OP_LOOKUP ? -2 : -1);  // -2: needs a lookup
-                    P.upsert_of.push_back(-1);
-                    g_lastw.push_back(0xFFFFFFFFu);
-                    g_key.push_back(k);
-                }
-                s.group[j] = g;
-                if (types[r] != HIVE_OP_LOOKUP) {
-                    if (g_lastw[g] == 0xFFFFFFFFu) ++nw;
-                    g_lastw[g] = (uint32_t)j;
-                }
-            }
-            for (size_t g = 0; g < P.find_of.size(); ++g) {
-                if (P.find_of[g] == -2) {
-                    P.find_of[g] = (int32_t)P.fkeys.size();
-                    P.fkeys.push_back(g_key[g]);
-                } else {
-                    P.find_of[g] = -1;
-                }
-                if (g_lastw[g] != 0xFFFFFFFFu) {
-                    const uint64_t r = s.first + g_lastw[g];
-                    P.upsert_of[g] = (int32_t)P.ukeys.size();
-                    P.ukeys.push_back(keys[r]);
-                    P.uvals.push_back(vals[r]);
-                }
-            }
-            P.new_writes = nw;
-        });
-        // the workers' lists, one after another, in the slot's pinned staging
+        // coalesce by key: a group whose first request is a lookup needs one device lookup; a group
+        // with writes needs one device upsert of its last written value; a lookup after a write of
+        // its key in the batch is answered from that write
+        gid.next_batch();
+        s.ans.resize(take);
+        g_key.clear();
+        g_lastw.clear();
+        g_look.clear();
         uint64_t new_writes = 0;
-        s.nf = s.nu = 0;
-        for (int w = 0; w < nparts; ++w) {
-            Part& P = s.parts[w];
-            P.f_off = s.nf;
-            P.u_off = s.nu;
-            s.nf += (uint32_t)P.fkeys.size();
-            s.nu += (uint32_t)P.ukeys.size();
-            new_writes += P.new_writes;
-        }
-        run_parts(nparts, [&](int w) {
-            const Part& P = s.parts[w];
-            if (!P.fkeys.empty()) std::memcpy(s.h_fkeys + P.f_off, P.fkeys.data(), P.fkeys.size() * 4);
-            if (!P.ukeys.empty()) {
-                std::memcpy(s.h_ukeys + P.u_off, P.ukeys.data(), P.ukeys.size() * 4);
-                std::memcpy(s.h_uvals + P.u_off, P.uvals.data(), P.uvals.size() * 4);
+        for (uint64_t j = 0; j < take; ++j) {
+            const uint64_t r = s.first + j;
+            bool added;
+            const int32_t g = gid.find_or_add(keys[r], (int32_t)g_key.size(), &added);
+            const bool lookup = types[r] == HIVE_OP_LOOKUP;
+            if (added) {
+                g_key.push_back(keys[r]);
+                g_lastw.push_back(-1);
+                g_look.push_back(lookup);
             }
-        });
+            if (lookup) {
+                s.ans[j] = g_lastw[g] >= 0 ? g_lastw[g] : -(g + 1);
+            } else {
+                if (g_lastw[g] < 0) ++new_writes;
+                g_lastw[g] = (int32_t)j;
+                s.ans[j] = -(g + 1);
+            }
+        }
+        const size_t ng = g_key.size();
+        s.fpos.resize(ng);
+        s.upos.resize(ng);
+        s.nf = s.nu = 0;
+        for (size_t g = 0; g < ng; ++g) {
+            if (g_look[g]) {
+                s.h_fkeys[s.nf] = g_key[g];
+                s.fpos[g] = (int32_t)s.nf++;
+            } else {
+                s.fpos[g] = -1;
+            }
+            if (g_lastw[g] >= 0) {
+                s.h_ukeys[s.nu] = g_key[g];
+                s.h_uvals[s.nu] = vals[s.first + g_lastw[g]];
+                s.upos[g] = (int32_t)s.nu++;
+            } else {
+                s.upos[g] = -1;
+            }
+        }
         // growth: keep the load factor under max_load counting every write in flight as a new key
         if (cfg->max_load > 0.0 && new_writes) {
             hive_get_info(t, &info);

@@ -24,8 +24,7 @@ MIXES = {"A": 0, "B": 1, "C": 2, "D": 3}  # 50/50 lookup/update, 95/5, 100 % loo
 
 class ServeConfig(ctypes.Structure):
     _fields_ = [("depth", ctypes.c_uint32), ("max_batch", ctypes.c_uint32), ("max_load", ctypes.c_double),
-                ("live_keys", ctypes.c_uint64), ("grow_start", ctypes.c_double), ("host_threads", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("live_keys", ctypes.c_uint64), ("grow_start", ctypes.c_double)]
 
 
 class ServeStats(ctypes.Structure):
@@ -104,11 +103,9 @@ class ServeResult:
 
 
 def serve(table: HiveHashTable, types, keys, vals, arrival, depth: int = 4, max_batch: int = 1 << 14,
-          max_load: float = 0.9, live_keys: Optional[int] = None, grow_start: Optional[float] = None,
-          host_threads: int = 0) -> ServeResult:
+          max_load: float = 0.9, live_keys: Optional[int] = None, grow_start: Optional[float] = None) -> ServeResult:
     """Run the request stream through the native loop.  Growth is incremental from `grow_start`
-    (default 0.8 * max_load; 0 = off, grow at once after a drain when max_load would be passed).
-    host_threads: workers that coalesce large batches (0 = automatic, 1 = the calling thread)."""
+    (default 0.8 * max_load; 0 = off, grow at once after a drain when max_load would be passed)."""
     types = np.ascontiguousarray(types, dtype=np.uint8)
     keys = np.ascontiguousarray(keys, dtype=np.uint32)
     vals = np.ascontiguousarray(vals, dtype=np.uint32)
@@ -119,8 +116,7 @@ def serve(table: HiveHashTable, types, keys, vals, arrival, depth: int = 4, max_
     done = np.zeros(n, dtype=np.float64)
     if grow_start is None:
         grow_start = 0.8 * max_load
-    cfg = ServeConfig(depth, max_batch, max_load, table.size() if live_keys is None else live_keys, grow_start,
-                      host_threads, 0)
+    cfg = ServeConfig(depth, max_batch, max_load, table.size() if live_keys is None else live_keys, grow_start)
     st = ServeStats()
     rc = lib().hive_serve_run(table.handle, ctypes.byref(cfg), types.ctypes.data, keys.ctypes.data, vals.ctypes.data,
                               arrival.ctypes.data, n, out_v.ctypes.data, out_s.ctypes.data, done.ctypes.data,

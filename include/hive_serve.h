@@ -37,9 +37,6 @@ typedef struct hive_serve_config {
     double max_load;     /* grow before a batch could pass this load factor (0 = never grow) */
     uint64_t live_keys;  /* keys already in the table when the run starts                   */
     double grow_start;   /* begin incremental growth at this load factor (0 = off; < max_load) */
-    uint32_t host_threads; /* host workers that coalesce and answer a batch of >= 4096 requests
-                              (0 = half the hardware threads, at most 8; 1 = the calling thread) */
-    uint32_t reserved;     /* 0 */
 } hive_serve_config;
 
 typedef struct hive_serve_stats {
