@@ -16,8 +16,10 @@
 //              upserts, on the single compute stream (batches therefore reach the table in
 //              arrival order); the results back on the copy stream
 //   pipeline   up to `depth` batches are in flight: while the GPU works on one, the next batch is
-//              formed, copied and queued.  depth = 1 is the plain loop: one synchronous batch at
-//              a time
+//              formed, copied and queued.  depth = 1 is the plain loop: one batch at a time
+//   answer     a second host thread takes the batches in order as their results reach the host
+//              and answers their requests, while this thread forms the next batch: a batch that
+//              finishes on the GPU is answered at once instead of after the next formation
 //   growth     the load is tracked without touching the device: keys known placed (from the
 //              statuses of finished batches) plus every distinct write in flight counted as new.
 //              Loads count against the slots of the unsplit level (8 n_lo; see level_slots).
@@ -35,10 +37,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "hive_serve.h"
@@ -116,7 +120,6 @@ struct Slot {
     std::vector<int32_t> fpos, upos;  // group -> position in the lookup / upsert list, or -1
     uint32_t nf = 0, nu = 0;
     uint64_t new_writes = 0;          // distinct written keys of the batch (possible new keys)
-    bool busy = false;
 };
 
 // Device bytes per bucket of a table allocation (8 slots, 8 stash entries, fingerprint word,
@@ -196,8 +199,12 @@ int hive_serve_run(
     for (auto& s : slots)
         if ((rc = alloc_slot(s, cap))) break;
     hive_info info{};
-    uint64_t live_done = cfg->live_keys;  // keys in the table after the finished batches
-    uint64_t pending_new = 0;             // possible new keys of the batches in flight
+    // shared with the answering thread
+    std::atomic<uint64_t> live_done{cfg->live_keys};  // keys in the table after the answered batches
+    std::atomic<uint64_t> pending_new{0};             // possible new keys of the batches in flight
+    std::atomic<uint64_t> launched{0}, answered{0};   // batches queued / answered (in order)
+    std::atomic<uint64_t> finished{0};                // requests answered
+    std::atomic<int> answer_rc{HIVE_OK};
     uint64_t grow_target = 0, grow_step = 0;  // incremental growth: target buckets, buckets per step
     uint64_t grow_refused_at = 0;             // bucket count at which growth found no memory
 
@@ -206,9 +213,7 @@ int hive_serve_run(
     std::vector<int32_t> g_lastw;   // group -> offset of its latest write so far, or -1
     std::vector<uint8_t> g_look;    // group -> its first request is a lookup
     // Requests are admitted in arrival order, so the pending ones are always [pend, next).
-    uint64_t pend = 0, next = 0, finished = 0;
-    size_t head = 0;                // ring position of the oldest in-flight slot
-    size_t in_flight = 0;
+    uint64_t pend = 0, next = 0;
     const auto t0 = Clock::now();
     auto now_s = [&] { return std::chrono::duration<double>(Clock::now() - t0).count(); };
 
@@ -235,42 +240,52 @@ int hive_serve_run(
         }
         uint64_t placed_new = 0;
         for (uint32_t u = 0; u < s.nu; ++u) placed_new += s.h_ust[u] == HIVE_ST_INSERTED || s.h_ust[u] == HIVE_ST_STASHED;
-        live_done += placed_new;
-        pending_new -= s.new_writes;
+        live_done.fetch_add(placed_new);
+        pending_new.fetch_sub(s.new_writes);
         const double td = now_s();
         std::fill(done_s + s.first, done_s + s.first + s.count, td);
-        finished += s.count;
-        s.busy = false;
         st.answer_s += now_s() - ta;
+        finished.fetch_add(s.count, std::memory_order_release);
     };
+
+    // The answering thread: takes the queued batches in order as their results reach the host and
+    // answers them, while this thread forms and queues the next ones (different batches write
+    // different output ranges).
+    std::atomic<bool> stop{false};
+    std::thread answerer([&] {
+        for (;;) {
+            const uint64_t a = answered.load(std::memory_order_acquire);
+            if (a < launched.load(std::memory_order_acquire)) {
+                Slot& s = slots[a % slots.size()];
+                cudaError_t q;
+                for (int spin = 0; (q = cudaEventQuery(s.done)) == cudaErrorNotReady; ++spin)
+                    if ((spin & 63) == 63) std::this_thread::yield();
+                if (q != cudaSuccess) {
+                    answer_rc.store(HIVE_ERR_CUDA);
+                    return;
+                }
+                finish(s);
+                answered.store(a + 1, std::memory_order_release);
+            } else if (stop.load(std::memory_order_acquire)) {
+                return;
+            } else {
+                std::this_thread::yield();
+            }
+        }
+    });
 
     auto drain = [&] {
-        while (in_flight) {
-            Slot& s = slots[head];
-            if (cudaEventSynchronize(s.done) != cudaSuccess) return HIVE_ERR_CUDA;
-            finish(s);
-            head = (head + 1) % slots.size();
-            --in_flight;
-        }
-        return HIVE_OK;
+        while (answered.load(std::memory_order_acquire) < launched.load(std::memory_order_relaxed))
+            if (answer_rc.load()) return answer_rc.load();
+        return answer_rc.load();
     };
 
-    size_t tail = 0;  // next slot to fill
-    while (!rc && finished < n) {
+    while (!rc && finished.load(std::memory_order_acquire) < n) {
+        if ((rc = answer_rc.load())) break;
         // admit arrivals
         const double tn = now_s();
         while (next < n && arrival_s[next] <= tn) ++next;
-        // retire completed batches in order
-        while (in_flight) {
-            Slot& s = slots[head];
-            const cudaError_t q = cudaEventQuery(s.done);
-            if (q == cudaErrorNotReady) break;
-            if (q != cudaSuccess) { rc = HIVE_ERR_CUDA; break; }
-            finish(s);
-            head = (head + 1) % slots.size();
-            --in_flight;
-        }
-        if (rc) break;
+        const uint64_t in_flight = launched.load(std::memory_order_relaxed) - answered.load(std::memory_order_acquire);
         if (pend == next || in_flight == slots.size()) {
             if (pend == next && next < n && in_flight == 0) {
                 // idle until the next arrival
@@ -282,7 +297,7 @@ int hive_serve_run(
         }
         // form a batch
         const double tf = now_s();
-        Slot& s = slots[tail];
+        Slot& s = slots[launched.load(std::memory_order_relaxed) % slots.size()];
         const uint64_t take = std::min<uint64_t>(next - pend, cap);
         s.first = pend;
         s.count = take;
@@ -421,11 +436,12 @@ int hive_serve_run(
         st.launch_s += now_s() - tl;
         st.device_lookups += s.nf;
         st.device_upserts += s.nu;
-        s.busy = true;
-        tail = (tail + 1) % slots.size();
-        ++in_flight;
+        launched.fetch_add(1, std::memory_order_release);
     }
     if (!rc) rc = drain();
+    stop.store(true, std::memory_order_release);
+    answerer.join();
+    if (!rc) rc = answer_rc.load();
     if (!rc) rc = hive_check(t, compute);
     st.wall_s = now_s();
     if (stats) *stats = st;
