@@ -64,6 +64,7 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-bucket ceiling probes")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-workload summary")
     ap.add_argument("--sharded", action="store_true",
                     help="bulk workload through the hash-partitioned table (exchange over NCCL) instead of replicas")
     ap.add_argument("--l2-window", type=int, choices=[0, 1, 2], default=None,
@@ -421,31 +422,63 @@ def run_served(args, dev):
 
     n_req = 1 << args.requests_log
     out = {"metric": "served requests: latency p50/p99/p999 (ms) at fractions of peak Mops/s", "unit": "ms",
-           "workload": f"2^26 records in 2^27 slots, Zipf 0.99, {n_req:,} requests per run, depth 4, batches <= 2^16",
+           "workload": f"2^26 records in 2^27 slots, Zipf 0.99, {n_req:,} requests per run, depth 4, batches <= 2^14",
            "higher_is_better": False, "mixes": {}}
     wu = ServedWorkload(5, 1 << 16, 1 << 16, "D")  # warm-up: kernel loading, first allocations
     with HiveHashTable(1 << 17) as t:
         t.insert(wu.preload_keys, wu.preload_vals)
-        serve(t, wu.types, wu.keys, wu.vals, poisson_arrivals(wu.keys.size, 0), depth=4, max_batch=1 << 16)
+        serve(t, wu.types, wu.keys, wu.vals, poisson_arrivals(wu.keys.size, 0), depth=4, max_batch=1 << 14)
     for mix in ("A", "B", "C", "D"):
         w = ServedWorkload(17, 1 << 26, n_req, mix)
         with HiveHashTable(1 << 27) as t:
             st = t.insert(w.preload_keys, w.preload_vals)
             torch_sync()
             assert bool((st != 0).all())
-            r = serve(t, w.types, w.keys, w.vals, poisson_arrivals(n_req, 0), depth=4, max_batch=1 << 16)
+            r = serve(t, w.types, w.keys, w.vals, poisson_arrivals(n_req, 0), depth=4, max_batch=1 << 14)
             peak = r.summary()["mops"]
             runs = {"peak": {k: round(v, 4) if isinstance(v, float) else v for k, v in r.summary().items()}}
             for frac in (0.1, 0.25, 0.5, 0.8, 0.9):
                 arr = poisson_arrivals(n_req, frac * peak * 1e6, seed=int(frac * 100))
-                s = serve(t, w.types, w.keys, w.vals, arr, depth=4, max_batch=1 << 16).summary()
+                s = serve(t, w.types, w.keys, w.vals, arr, depth=4, max_batch=1 << 14).summary()
                 runs[f"{frac:.2f}"] = {k: round(s[k], 4) for k in ("mops", "p50_ms", "p99_ms", "p999_ms")}
             # the plain loop at the same offered load: one batch at a time (depth 1), so requests
             # that arrive while a batch is on the GPU wait for it to finish
             arr = poisson_arrivals(n_req, 0.8 * peak * 1e6, seed=80)
-            s = serve(t, w.types, w.keys, w.vals, arr, depth=1, max_batch=1 << 16).summary()
+            s = serve(t, w.types, w.keys, w.vals, arr, depth=1, max_batch=1 << 14).summary()
             runs["0.80_plain_depth1"] = {k: round(s[k], 4) for k in ("mops", "p50_ms", "p99_ms", "p999_ms")}
             out["mixes"][mix] = runs
+            t.check()
+    return out
+
+
+def served_summary(dev, n_req=1 << 20, max_batch=1 << 14):
+    """The served workload in brief for the headline line: per mix (A 50/50 lookup/update, B 95/5,
+    C lookups, D 95 % lookups / 5 % new inserts; Zipf 0.99 over 2^26 preloaded records in 2^27
+    slots), the closed-loop peak of the continuous loop (depth 4), then Poisson arrivals at 80 % of
+    that peak through the continuous loop and through the plain loop (depth 1, one batch at a
+    time), with p50 / p99 / p999 latency from arrival to result on the host."""
+    import torch
+    from hivehashtable_b200 import HiveHashTable
+    from hivehashtable_b200.serving import ServedWorkload, poisson_arrivals, serve
+
+    out = {"requests_per_run": n_req, "max_batch": max_batch, "mixes": {}}
+    with HiveHashTable(1 << 27) as t:
+        for mix in ("A", "B", "C", "D"):
+            w = ServedWorkload(17, 1 << 26, n_req, mix)
+
+            def run(arr, depth):
+                t.clear()
+                t.insert(w.preload_keys, w.preload_vals)
+                torch.cuda.synchronize()
+                return serve(t, w.types, w.keys, w.vals, arr, depth=depth, max_batch=max_batch).summary()
+
+            run(poisson_arrivals(n_req, 0), 4)  # warm-up
+            peak = run(poisson_arrivals(n_req, 0), 4)["mops"]
+            row = {"peak_mops": round(peak, 2)}
+            for name, depth in (("continuous_80", 4), ("plain_80", 1)):
+                r = run(poisson_arrivals(n_req, 0.8 * peak * 1e6, seed=80), depth)
+                row[name] = {k: round(r[k], 4) for k in ("mops", "p50_ms", "p99_ms", "p999_ms")}
+            out["mixes"][mix] = row
             t.check()
     return out
 
@@ -768,6 +801,11 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(args)
+    served = None
+    if rank == 0 and world == 1 and not args.no_served:
+        table.close()
+        torch.cuda.empty_cache()
+        served = served_summary(dev)
     ceiling = None
     if rank == 0 and not args.no_probe:
         ceiling = random_bucket_ceiling(dev, cap * 8)
@@ -816,7 +854,7 @@ def main():
                 "config": workload_config(args, world), "roofline": roof, "roofline_all": rl,
                 "insert_mops": rl["k_insert"]["mops"], "lookup_mops": rl["k_find"]["mops"],
                 "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches_per_step(cap, n, n_look) * args.steps,
-                "insert_counters": step_counters, "random_bucket_ceiling": ceiling,
+                "insert_counters": step_counters, "random_bucket_ceiling": ceiling, "served": served,
                 "clocks": sampler.summary()}
         print(json.dumps(line), flush=True)
     table.close()
