@@ -90,6 +90,9 @@ constexpr uint32_t kFlagHandOn = 16u;  // set on the launch's copy only: a locke
                                       // pass that finishes such ops together
 constexpr uint32_t kFlagResumed = 32u;     // set on the launch's copy only: the ops were counted
                                            // on the slow path by the pass that handed them on
+constexpr uint32_t kFlagMigrating = 64u;   // set on the launch's copy only: the same launch splits
+                                           // buckets [split, win_end) of the level while its ops
+                                           // run (see in_window)
 
 // The device view of a table, passed to every kernel by value.
 //
@@ -111,6 +114,7 @@ struct Table {
     uint32_t split;
     uint32_t max_evictions;
     uint32_t flags;
+    uint32_t win_end;  // with kFlagMigrating: the window being split is [split, win_end)
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -198,6 +202,15 @@ __device__ __forceinline__ uint32_t bucket_addr(const Table& t, uint32_t h) {
     if (b < t.split) b = fastmod(h, t.m_hi, t.n_lo << 1);
     return b;
 }
+
+// Whether hash h addresses a bucket of the window that the running launch is splitting: such a
+// key may sit in its old home b = h mod n_lo or its new one, h mod 2 n_lo (b or b + n_lo).
+__device__ __forceinline__ bool in_window(const Table& t, uint32_t h) {
+    if (!(t.flags & kFlagMigrating)) return false;
+    const uint32_t b = fastmod(h, t.m_lo, t.n_lo);
+    return b >= t.split && b < t.win_end;
+}
+__device__ __forceinline__ uint32_t new_home(const Table& t, uint32_t h) { return fastmod(h, t.m_hi, t.n_lo << 1); }
 
 // ---------------------------------------------------------------------------------------------
 // Bucket access
@@ -639,8 +652,14 @@ __device__ __forceinline__ bool find_tagged(const Table& t, uint32_t b, u64 T, u
 template <int P, bool kReadOnly>
 __device__ __forceinline__ bool find_one_buckets(const Table& t, uint32_t k, uint32_t* v);
 
+template <int P>
+__device__ __noinline__ bool find_one_migrating(const Table& t, uint32_t k, uint32_t* v);
+
 template <int P, bool kReadOnly>
 __device__ __forceinline__ bool find_one(const Table& t, uint32_t k, uint32_t* v) {
+    if (!kReadOnly && (t.flags & kFlagMigrating) &&
+        (in_window(t, Policy<P>::h0(k)) || in_window(t, Policy<P>::h1(k))))
+        return find_one_migrating<P>(t, k, v);
     if (t.flags & kFlagUntagged) return find_one_buckets<P, kReadOnly>(t, k, v);
     if (k == 0) return false;
     const uint32_t f = tag_of(k);
@@ -689,6 +708,65 @@ __device__ __forceinline__ bool find_one_buckets(const Table& t, uint32_t k, uin
     }
     *v = val_of(slot_at(B, __ffs(m) - 1));
     return true;
+}
+
+// Lookup of a key with a candidate bucket in the window being split by the running launch.  The
+// splitter writes a bucket's new home (and the new home's stash) before it clears what moved
+// out of the old one, so reading each old home before its new home, and the old stash before the
+// new, always finds a key that is present (whole buckets: the tag words of the window are
+// rewritten by the splitter).  Keys of the window are not evicted during such a launch and no
+// key is evicted into it, so the H0-then-H1 order needs nothing more.
+template <int P>
+__device__ __noinline__ bool find_one_migrating(const Table& t, uint32_t k, uint32_t* v) {
+    if (k == 0) return false;
+    uint32_t homes[5];
+    int nh = 0;
+    const uint32_t hs[2] = {Policy<P>::h0(k), Policy<P>::h1(k)};
+#pragma unroll
+    for (int x = 0; x < 2; ++x) {
+        if (in_window(t, hs[x])) {
+            const uint32_t b = fastmod(hs[x], t.m_lo, t.n_lo), b2 = new_home(t, hs[x]);
+            homes[nh++] = b;
+            if (b2 != b) homes[nh++] = b2;
+        } else {
+            homes[nh++] = bucket_addr(t, hs[x]);
+        }
+    }
+    Bucket B;
+    for (int x = 0; x < nh; ++x) {
+        load_bucket(t.slots + (size_t)homes[x] * kSlots, B);
+        const uint32_t m = match_mask(B, k);
+        if (m) {
+            *v = val_of(slot_at(B, __ffs(m) - 1));
+            return true;
+        }
+    }
+    // the canonical stash: old, then new
+    uint32_t c[2];
+    int nc = 0;
+    if (in_window(t, hs[0])) {
+        c[nc++] = fastmod(hs[0], t.m_lo, t.n_lo);
+        if (new_home(t, hs[0]) != c[0]) c[nc++] = new_home(t, hs[0]);
+    } else {
+        c[nc++] = bucket_addr(t, hs[0]);
+    }
+    for (int x = 0; x < nc; ++x) {
+        if (!stash_flag(t, c[x])) continue;
+        load_bucket(t.stash + (size_t)c[x] * kSlots, B);
+        const uint32_t m = match_mask(B, k);
+        if (m) {
+            *v = val_of(slot_at(B, __ffs(m) - 1));
+            return true;
+        }
+    }
+    return false;
+}
+
+// Whether an op on key k would write into the window being split (its candidate buckets, or its
+// canonical stash): such writes wait until the window is done.
+template <int P>
+__device__ __forceinline__ bool touches_window(const Table& t, uint32_t k) {
+    return in_window(t, Policy<P>::h0(k)) || in_window(t, Policy<P>::h1(k));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -776,8 +854,9 @@ __device__ __forceinline__ int try_evict(const Table& t, u64* B0p, const Bucket&
             }
             const uint32_t vk = key_of(vkv);
             if (bucket_addr(t, Policy<P>::h0(vk)) != b0) continue;  // victim lives in its H1
-            const uint32_t alt = bucket_addr(t, Policy<P>::h1(vk));
-            if (alt == b0) continue;
+            const uint32_t h1 = Policy<P>::h1(vk);
+            const uint32_t alt = bucket_addr(t, h1);
+            if (alt == b0 || in_window(t, h1)) continue;  // no victim moves into a window being split
             alts[q] = alt;
             cand |= 1u << q;
         }

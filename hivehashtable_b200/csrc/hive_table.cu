@@ -967,6 +967,132 @@ __global__ void k_split(hive::Table told, hive::Table tnew, uint32_t s, uint32_t
     if (nd == hive::kSlots) hive::mark_full(told, nbk);
 }
 
+// Split of bucket b of the window [told.split, told.win_end) while other ops of the launch read
+// the table (k_apply_split).  Readers of a window key read its old home b before its new home
+// nbk = b + n_lo and b's stash before nbk's (find_one_migrating), so the entries that move are
+// written to their new places first and only then, after a fence, removed from the old ones.
+// Entries that stay keep their positions (a reader reads a bucket in two halves), and stash
+// entries stay stash entries (a stash entry moved into a slot could be passed by a reader that
+// reads the slots before the stash).  No op of the launch writes into the window.
+template <int P>
+__device__ void split_bucket_live(const hive::Table& told, const hive::Table& tnew, uint32_t b) {
+    const uint32_t nbk = b + told.n_lo;
+    u64* src = told.slots + (size_t)b * hive::kSlots;
+    u64* dst = told.slots + (size_t)nbk * hive::kSlots;
+    const bool tags = !(told.flags & hive::kFlagUntagged);
+    hive::Bucket B;
+    hive::load_bucket(src, B);
+    u64 moved[hive::kSlots];
+    uint32_t out = 0;  // bit j: slot j of b moves
+    int nd = 0;
+#pragma unroll
+    for (int j = 0; j < hive::kSlots; ++j) moved[j] = 0ull;
+#pragma unroll
+    for (int j = 0; j < hive::kSlots; ++j) {
+        const u64 kv = B.s[j];
+        if (!kv) continue;
+        bool via0;
+        const uint32_t h = resident_hash<P>(told, hive::key_of(kv), b, &via0);
+        if (hive::bucket_addr(tnew, h) == nbk) {
+            moved[nd++] = kv;
+            out |= 1u << j;
+        }
+    }
+    const bool has_stash = (told.stash_bits[b >> 5] >> (b & 31)) & 1u;
+    hive::Bucket S;
+    uint32_t sout = 0;
+    int nms = 0, nks = 0;
+    u64* sb = told.stash + (size_t)b * hive::kSlots;
+    u64* sn = told.stash + (size_t)nbk * hive::kSlots;
+    if (has_stash) {
+        hive::load_bucket(sb, S);
+        for (int j = 0; j < hive::kSlots; ++j) {
+            const u64 kv = S.s[j];
+            if (!kv) continue;
+            if (hive::bucket_addr(tnew, hive::Policy<P>::h0(hive::key_of(kv))) == nbk) sout |= 1u << j;
+            else ++nks;
+        }
+    }
+    // 1. the new homes: nbk's slots and stash (and its flag, before any entry leaves b's stash)
+#pragma unroll
+    for (int j = 0; j < hive::kSlots; ++j) dst[j] = moved[j];
+    if (sout) {
+        for (int j = 0; j < hive::kSlots; ++j) sn[j] = (sout >> j) & 1u ? S.s[j] : 0ull;
+        atomicOr(told.stash_bits + (nbk >> 5), 1u << (nbk & 31));
+    }
+    if (tags) told.tags[nbk] = hive::tag_word(moved);
+    if (nd == hive::kSlots) hive::mark_full(told, nbk);
+    __threadfence();
+    // 2. the old home loses what moved
+    u64 keep[hive::kSlots];
+    int nk = 0;
+#pragma unroll
+    for (int j = 0; j < hive::kSlots; ++j) {
+        keep[j] = (out >> j) & 1u ? 0ull : B.s[j];
+        nk += keep[j] != 0ull;
+        if ((out >> j) & 1u) src[j] = 0ull;
+    }
+    if (sout) {
+        for (int j = 0; j < hive::kSlots; ++j)
+            if ((sout >> j) & 1u) sb[j] = 0ull;
+        if (!nks) atomicAnd(told.stash_bits + (b >> 5), ~(1u << (b & 31)));
+    }
+    if (tags) told.tags[b] = hive::tag_word(keep);
+    if (nk == hive::kSlots) hive::mark_full(told, b);
+    else hive::mark_not_full(told, b);
+}
+
+// A batch of mixed ops while the same launch splits the window [tmig.split, tmig.win_end) (a
+// cooperative launch: every block is resident).  Phase 1: threads split the window's buckets,
+// one bucket each, while all threads run the batch's ops against the table as it is being split
+// (tmig): lookups read both homes of a window key; ops that would write into the window, and
+// inserts that need the locked path, are queued.  Grid barrier.  Phase 2: the queued ops, against
+// the split geometry (tnew), with the whole protocol.  Ops of one launch are unordered, so running
+// some after the barrier changes no result.
+template <int P, int kMode>
+__global__ void k_apply_split(hive::Table tmig, hive::Table tnew, const uint8_t* __restrict__ types,
+                              const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, uint64_t n,
+                              uint8_t* __restrict__ status, uint32_t* __restrict__ outv, uint32_t* q, u64* qn) {
+    cg::grid_group grid = cg::this_grid();
+    const u64 tid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t w_lo = tmig.split, w_cnt = tmig.win_end - tmig.split;
+    for (u64 x = tid; x < w_cnt; x += stride) split_bucket_live<P>(tmig, tnew, w_lo + (uint32_t)x);
+    const Defer d{q, qn};
+    for (u64 base = tid - lane; base < n; base += stride) {
+        const u64 i = base + lane;
+        const bool active = i < n;
+        uint32_t o = 0;
+        uint8_t st = 0;
+        bool later = false;
+        if (active) {
+            const uint8_t type = types[i];
+            const uint32_t k = keys[i];
+            if (type != HIVE_OP_LOOKUP && hive::touches_window<P>(tmig, k)) {
+                later = true;
+            } else {
+                st = apply_one<P, true, kMode>(tmig, type, k, vals ? vals[i] : 0u, &o);
+                later = st == hive::kStDefer;
+            }
+        }
+        defer_push(d, later, i);
+        if (active && !later) {
+            if (status) status[i] = st;
+            if (outv) outv[i] = o;
+        }
+    }
+    grid.sync();
+    const u64 cnt = *qn;
+    for (u64 j = tid; j < cnt; j += stride) {
+        const uint32_t i = q[j];
+        uint32_t o = 0;
+        const uint8_t st = apply_one<P, false, hive::kModeRuntime>(tnew, types[i], keys[i], vals ? vals[i] : 0u, &o);
+        if (status) status[i] = st;
+        if (outv) outv[i] = o;
+    }
+}
+
 // told: geometry before (buckets [lo, lo + cnt) + n_lo are folded); tnew: after.
 // Entries that find no room are appended to ovf for re-insertion.
 template <int P>
@@ -1835,6 +1961,48 @@ int hive_apply_batches(hive_table* h, const uint8_t* types, const uint32_t* keys
     void* args[] = {(void*)&tv, (void*)&types, (void*)&keys, (void*)&values, (void*)&offsets, (void*)&n_batches,
                     (void*)&status, (void*)&out_values, (void*)&d.q, (void*)&qn};
     HIVE_CUDA(cudaLaunchCooperativeKernel(fn, grid, block, args, 0, s));
+    return HIVE_OK;
+}
+
+int hive_apply_ops_split(hive_table* h, const uint8_t* types, const uint32_t* keys, const uint32_t* values,
+                         uint64_t n, uint8_t* status, uint32_t* out_values, uint32_t hints, uint64_t split_buckets,
+                         void* stream) {
+    if (!valid_table(h)) return HIVE_ERR_INVALID_ARG;
+    if (n && (!types || !keys)) return HIVE_ERR_INVALID_ARG;
+    if (n > 0xFFFFFFFFull) return HIVE_ERR_INVALID_ARG;
+    DeviceGuard g(h->device);
+    if (!g.ok) return HIVE_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    L2Window l2w(h, s);
+    const uint32_t sp = h->t.split, nlo = h->t.n_lo;
+    const uint32_t w = (uint32_t)std::min<uint64_t>(split_buckets, (uint64_t)(nlo - sp));
+    if (w == 0) return n ? hive_apply_ops(h, types, keys, values, n, status, out_values, hints, stream) : HIVE_OK;
+    int rc = grow_capacity(h, (uint64_t)nlo + sp + w, s);
+    if (rc) return rc;
+    h->t.flags |= hive::kFlagHoles;  // entries leave their buckets
+    Defer d;
+    if ((rc = prepare_defer(h, std::max<uint64_t>(n, 1), s, &d))) return rc;
+    hive::Table tv;
+    if ((rc = table_view(h, s, &tv))) return rc;
+    hive::Table tmig = tv, tnew = tv;
+    tmig.flags |= hive::kFlagMigrating;
+    tmig.win_end = sp + w;
+    tnew.split = sp + w;  // split == n_lo addresses exactly as the next level with split 0
+    HIVE_CUDA(cudaMemsetAsync(d.n, 0, 8, s));
+    const bool p1 = h->policy == HIVE_POLICY_MURMURCITYHASH;
+    const bool uniq = hints & HIVE_HINT_UNIQUE_KEYS;
+    constexpr int kHU = hive::kModeHoles | hive::kModeUnique;
+    const void* fn = p1 ? (uniq ? (const void*)k_apply_split<1, kHU> : (const void*)k_apply_split<1, hive::kModeHoles>)
+                        : (uniq ? (const void*)k_apply_split<0, kHU> : (const void*)k_apply_split<0, hive::kModeHoles>);
+    int fit = 0;
+    HIVE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, kBlock, 0));
+    if (fit < 1) return HIVE_ERR_INVALID_ARG;
+    dim3 grid((unsigned)(fit * h->num_sms)), block((unsigned)kBlock);
+    void* args[] = {(void*)&tmig, (void*)&tnew, (void*)&types, (void*)&keys, (void*)&values, (void*)&n,
+                    (void*)&status, (void*)&out_values, (void*)&d.q, (void*)&d.n};
+    HIVE_CUDA(cudaLaunchCooperativeKernel(fn, grid, block, args, 0, s));
+    if (sp + w == nlo) set_geometry(h, h->level + 1, 0);
+    else set_geometry(h, h->level, sp + w);
     return HIVE_OK;
 }
 

@@ -87,6 +87,7 @@ ABI = [
     ("hive_erase", _I32, [_P, _P, _U64, _P, _P]),
     ("hive_apply_ops", _I32, [_P, _P, _P, _P, _U64, _P, _P, _U32, _P]),
     ("hive_apply_reference_ops", _I32, [_P, _P, _U64, _P, _U32, _P]),
+    ("hive_apply_ops_split", _I32, [_P, _P, _P, _P, _U64, _P, _P, _U32, _U64, _P]),
     ("hive_apply_batches", _I32, [_P, _P, _P, _P, _P, _U32, _U64, _P, _P, _U32, _I32, _I32, _P]),
     ("hive_size", _I32, [_P, ctypes.POINTER(_U64), _P]),
     ("hive_dump", _I32, [_P, _P, _U64, ctypes.POINTER(_U64), _P]),
@@ -304,6 +305,20 @@ class HiveHashTable:
         outv = torch.empty(n, dtype=torch.int32, device=self.device)
         _check(self._lib.hive_apply_ops(self._h, _ptr(t), _ptr(k), _ptr(v), n, _ptr(status), _ptr(outv),
                                         hints, self._stream(stream)), "hive_apply_ops")
+        return status, outv
+
+    def apply_split(self, types, keys, values=None, split_buckets: int = 0, hints: int = 0,
+                    stream=None) -> Tuple[torch.Tensor, torch.Tensor]:
+        """apply() while the same launch splits the next `split_buckets` buckets of the current
+        level (hive_apply_ops_split): the table grows while the batch runs."""
+        t = as_device_u8(types, self.device)
+        k = as_device_u32(keys, self.device)
+        v = None if values is None else as_device_u32(values, self.device)
+        n = k.numel()
+        status = torch.empty(n, dtype=torch.uint8, device=self.device)
+        outv = torch.empty(n, dtype=torch.int32, device=self.device)
+        _check(self._lib.hive_apply_ops_split(self._h, _ptr(t), _ptr(k), _ptr(v), n, _ptr(status), _ptr(outv), hints,
+                                              int(split_buckets), self._stream(stream)), "hive_apply_ops_split")
         return status, outv
 
     def apply_batches(self, types: torch.Tensor, keys: torch.Tensor, values: Optional[torch.Tensor],

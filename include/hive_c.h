@@ -200,6 +200,20 @@ int hive_apply_batches(hive_table* t, const uint8_t* types, const uint32_t* keys
                        uint32_t* out_values, uint32_t hints, int threads_per_block, int blocks_per_sm,
                        void* stream);
 
+/* hive_apply_ops while the same launch splits the next `split_buckets` buckets of the table's
+ * current level (linear hashing: bucket b moves the keys that now address b + n_lo), so the
+ * table grows while its ops run.  Lookups of keys whose bucket is being split read both its old
+ * and its new home; ops that would write into those buckets, and inserts that need the locked
+ * path, finish after the split, in the same launch.  Results are those of hive_apply_ops; the
+ * geometry (hive_get_info) has advanced by min(split_buckets, buckets left in the level) when the
+ * call returns.  Grows the allocation first (synchronously) when it lacks room.  A cooperative
+ * launch.  Replaces the reference's grow between launches (hive_hash_grow,
+ * include/hive_hash_resize.cuh:138-215, triggered at src/hive_dispatch.cu:181-211), which moves
+ * buckets only while no op runs. */
+int hive_apply_ops_split(hive_table* t, const uint8_t* types, const uint32_t* keys, const uint32_t* values,
+                         uint64_t n, uint8_t* status, uint32_t* out_values, uint32_t hints, uint64_t split_buckets,
+                         void* stream);
+
 /* Mixed batch in the reference's own record layout: ops points to n 16-byte records
  * {int32 type (OperationType); 4 bytes padding; uint64 key} (include/utils.h:18-21);
  * value = (uint32)key + 1 (include/hive_kernels.cuh:156); results[i] = 1 on success else 0,
