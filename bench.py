@@ -485,13 +485,16 @@ def served_summary(dev, n_req=1 << 20, max_batch=1 << 14):
 
 def run_resize(args, dev):
     """Growth and shrink (seed 13): a 2^20-slot table takes 2^27 unique keys in 128 chunks of
-    2^20 inserts, each followed by 2^17 lookups of inserted keys, doubling (linear-hashing splits)
-    before a chunk would pass LF 0.85; then 75 % of the keys are deleted in random order in chunks of
-    2^20, shrinking whenever the load falls below 0.25 by whole levels (halving while the keys fit
-    the half at LF 0.75).  Device time of each phase with its resizes included."""
+    2^20 inserts, each followed by 2^17 lookups of inserted keys, doubling (linear-hashing splits,
+    queued on the stream) before a chunk would pass LF 0.85; then 75 % of the keys are deleted in
+    random order in chunks of 2^20, shrinking whenever the load falls below 0.25 by whole levels
+    (halving while the keys fit the half at LF 0.75).  The growth and shrink points follow from the
+    known key counts, so the loop issues its calls without reading anything back; every lookup's
+    found flag lands in one buffer, counted at the end.  Device time of each phase, its resizes
+    included."""
     import numpy as np
     import torch
-    from hivehashtable_b200 import HiveHashTable, as_device_u32
+    from hivehashtable_b200 import HiveHashTable, as_device_u32, library
     from hivehashtable_b200 import workload
 
     n, chunk = 1 << 27, 1 << 20
@@ -503,11 +506,18 @@ def run_resize(args, dev):
     gone = as_device_u32(keys[order[: 3 * n // 4]], dev)
     look_idx = torch.from_numpy(np.random.default_rng(14).integers(0, chunk, size=chunk // 8)).to(dev)
     looks = kd.view(-1, chunk)[:, look_idx].contiguous()  # 2^17 inserted keys per chunk
+    n_look = looks.shape[1]
+    found = torch.zeros(looks.numel(), dtype=torch.uint8, device=dev)
+    status = torch.empty(chunk, dtype=torch.uint8, device=dev)
+    fvals = torch.empty(n_look, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    lib = library()
     out = {"metric": "resize: inserts with growth, deletes with shrink (Mops/s)", "unit": "Mops/s",
            "workload": "2^20 slots -> 2^27 keys in 128 chunks of 2^20 (+2^17 lookups each); delete 75 % in chunks",
            "higher_is_better": True}
     with HiveHashTable(1 << 20, max_capacity=1 << 29) as t:
+        h = t.handle
         # warm-up on this table, then clear: kernel loading and the table's own first allocations
         # (deferred-op queue, merge overflow buffer)
         t.insert(kd[:chunk], vd[:chunk])
@@ -518,113 +528,51 @@ def run_resize(args, dev):
         t.clear()
         torch.cuda.synchronize()
         grows = 0
-        missing = torch.zeros((), dtype=torch.int64, device=dev)
+        cap = 1 << 20
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         for c in range(n // chunk):
             live = c * chunk
-            cap = t.info()["capacity_slots"]
-            while (live + chunk) > 0.85 * cap:
-                cap *= 2
-            if cap != t.info()["capacity_slots"]:
-                t.resize(cap)
+            if (live + chunk) > 0.85 * cap:
+                while (live + chunk) > 0.85 * cap:
+                    cap *= 2
+                assert lib.hive_resize(h, cap, s) == 0
                 grows += 1
-            t.insert(kd[c * chunk:(c + 1) * chunk], vd[c * chunk:(c + 1) * chunk])
-            _, f = t.find(looks[c])
-            missing += (f == 0).sum()
+            assert lib.hive_insert(h, kd.data_ptr() + 4 * c * chunk, vd.data_ptr() + 4 * c * chunk, chunk,
+                                   status.data_ptr(), s) == 0
+            assert lib.hive_find(h, looks[c].data_ptr(), n_look, fvals.data_ptr(), found.data_ptr() + c * n_look,
+                                 s) == 0
         b.record(stream)
         torch.cuda.synchronize()
         ins_ms = a.elapsed_time(b)
+        missing = int((found == 0).sum().item())
         size_after_insert = t.size()
         shrinks = 0
         a.record(stream)
         for c in range(0, gone.numel(), chunk):
-            t.erase(gone[c:c + chunk])
-            live = n - min(c + chunk, gone.numel())
-            cap = t.info()["capacity_slots"]
+            m = min(chunk, gone.numel() - c)
+            assert lib.hive_erase(h, gone.data_ptr() + 4 * c, m, status.data_ptr(), s) == 0
+            live = n - (c + m)
             if live < 0.25 * cap:
                 # whole levels: halve while the entries fit the half at LF 0.75
                 tgt = cap
                 while tgt // 2 >= 1 << 20 and live <= 0.75 * (tgt // 2):
                     tgt //= 2
                 if tgt != cap:
-                    t.resize(tgt)
+                    assert lib.hive_resize(h, tgt, s) == 0
+                    cap = tgt
                     shrinks += 1
         b.record(stream)
         torch.cuda.synchronize()
         del_ms = a.elapsed_time(b)
         out.update({"insert_mops": round(n / ins_ms / 1e3, 1), "insert_ms": round(ins_ms, 2), "grows": grows,
-                    "lookups_missing": int(missing.item()), "size_after_insert": size_after_insert,
+                    "lookups_missing": missing, "size_after_insert": size_after_insert,
                     "delete_mops": round(gone.numel() / del_ms / 1e3, 1), "delete_ms": round(del_ms, 2),
                     "shrinks": shrinks, "size_after_delete": t.size(),
                     "final_capacity_slots": t.info()["capacity_slots"]})
         out["value"] = out["insert_mops"]
         t.check()
     return out
-
-
-def run_sharded(args, rank, world, local, dev):
-    """The hash-partitioned table (hivehashtable_b200/sharded.py): each of the N ranks holds a
-    2^cap_log-slot shard and submits its own n = LF * 2^cap_log keys (seed 7 + 1000 * rank); one
-    step = clear every shard, sharded bulk insert, sharded bulk lookup (present fraction as the
-    headline), each through the owner exchange (all_to_all_single over NCCL, also at N = 1).
-    Weak scaling: value = 2 n N / the slowest rank's time."""
-    import numpy as np
-    import torch
-    import torch.distributed as dist
-    from datetime import timedelta
-
-    from hivehashtable_b200 import HiveHashTable, as_device_u32, workload
-    from hivehashtable_b200.sharded import ShardedHiveTable
-
-    if not dist.is_initialized():
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        os.environ.setdefault("MASTER_PORT", "29517")
-        dist.init_process_group("nccl", rank=rank, world_size=world, timeout=timedelta(seconds=300), device_id=dev)
-    cap = 1 << args.cap_log
-    n = int(args.lf * cap)
-    keys_h, vals_h, look_h = workload.bulk_workload(args.seed + 1000 * rank, n, args.present)
-    keys, vals, look = as_device_u32(keys_h, dev), as_device_u32(vals_h, dev), as_device_u32(look_h, dev)
-    shard = HiveHashTable(cap, args.policy)
-    tbl = ShardedHiveTable(shard, dev)
-    stream = torch.cuda.current_stream(dev)
-
-    def step():
-        shard.clear()
-        st = tbl.insert(keys, vals)
-        _, f = tbl.find(look)
-        return st, f
-
-    for _ in range(args.warmup):
-        st, f = step()
-    torch.cuda.synchronize()
-    assert bool((st != 0).all()) and int(f.sum()) == int(round(look_h.size * args.present))
-    dist.barrier()
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(args.steps):
-        step()
-    b.record(stream)
-    torch.cuda.synchronize()
-    ms = torch.tensor([a.elapsed_time(b)], device=dev, dtype=torch.float64)
-    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-    ms = float(ms.item())
-    line = None
-    if rank == 0:
-        line = {"metric": METRIC + " (sharded table)", "value": round(2 * n * world * args.steps / (ms / 1e3) / 1e6, 2),
-                "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seeded uint32 keys/values)",
-                "config": dict(workload_config(args, world),
-                               parallelism=f"sharded: {world} rank(s), one 2^{args.cap_log}-slot shard each; owner = "
-                                           "(fmix32(key ^ 0x9E3779B9) * N) >> 32; one all_to_all_single of 9-byte "
-                                           "records out and 5-byte results back per call (NCCL)"),
-                "exchange_bytes_per_op": {"out": 9, "back": 5}}
-    shard.close()
-    dist.barrier()
-    dist.destroy_process_group()
-    return line
 
 
 def workload_config(args, world):
