@@ -10,9 +10,17 @@ settings of a table, so the tuner measures them on the device instead:
   region_insert        0, 2                         submission order vs one region-ordered pass
   second_pass_blocks   2, 4, 8                      resident blocks per SM of the deferred pass
   max_evictions        4, 8                         cuckoo victims tried per insert (a table setting)
+  stash_depth          8, 4                         canonical-stash slots an insert may use
+  l2_window            0, 1                         L2 persistence window over tables that fit it
 
-Bucket width (8 slots) and the stash size (8 per canonical bucket) are part of the table's
-semantics and are not tuned; one thread runs one op (no warps-per-op setting).
+The bucket width is not tuned: a bucket is one 64 B line, two 32 B sectors that a lane pair reads
+with one request, and its per-slot fingerprints are one 8-byte word; every kernel is built on that
+layout.  One thread runs one op (a lane pair shares each bucket read), so there is no warps-per-op
+setting either.
+
+A tuned setting is applied to new tables: HiveHashTable(..., tuning="cache") or the
+HIVE_TUNE_CACHE environment variable (the JSON file autotune() writes) picks the entry of the same
+GPU and policy whose capacity is nearest (lookup_cached).
 
 Search: coordinate descent from the defaults, one knob at a time, two rounds at most.  A setting
 is accepted only if it places every key the defaults place (no new failed inserts) and every lookup
@@ -25,8 +33,10 @@ import json
 from pathlib import Path
 from typing import Callable, Dict, Optional
 
-DEFAULTS = {"tags": 1, "region_insert": 0, "second_pass_blocks": 4, "max_evictions": 8}
-SPACE = {"tags": [1, 0, 2], "region_insert": [0, 2], "second_pass_blocks": [4, 2, 8], "max_evictions": [8, 4]}
+DEFAULTS = {"tags": 1, "region_insert": 0, "second_pass_blocks": 4, "max_evictions": 8, "stash_depth": 8,
+            "l2_window": 0}
+SPACE = {"tags": [1, 0, 2], "region_insert": [0, 2], "second_pass_blocks": [4, 2, 8], "max_evictions": [8, 4],
+         "stash_depth": [8, 4], "l2_window": [0, 1]}
 
 # measure(setting) -> {"ms": float, "failed": int, "correct": bool}
 Measure = Callable[[Dict[str, int]], Dict[str, float]]
@@ -84,7 +94,7 @@ def device_measure(capacity: int, load_factor: float, present: float = 0.5, poli
 
     def measure(setting):
         knobs = {k: v for k, v in setting.items() if k != "max_evictions"}
-        with HiveHashTable(capacity, policy, max_evictions=setting.get("max_evictions", 8)) as t:
+        with HiveHashTable(capacity, policy, max_evictions=setting.get("max_evictions", 8), tuning={}) as t:
             t.set_tuning(**knobs)
             times = []
             for it in range(warmup + reps):
@@ -133,6 +143,21 @@ def autotune(capacity: int, load_factor: float, present: float = 0.5, policy: st
         stored[key] = result
         Path(cache).write_text(json.dumps(stored, indent=1))
     return result
+
+
+def lookup_cached(cache: Path, gpu: str, capacity: int, policy: str) -> Optional[Dict[str, int]]:
+    """The best setting stored in `cache` for this GPU and policy at the capacity nearest to
+    `capacity` (in log2), or None."""
+    import math
+
+    if not cache or not Path(cache).exists():
+        return None
+    stored = json.loads(Path(cache).read_text())
+    cands = [r for r in stored.values() if r.get("gpu") == gpu and r.get("policy") == policy and "best" in r]
+    if not cands:
+        return None
+    r = min(cands, key=lambda e: abs(math.log2(e["capacity_slots"]) - math.log2(max(capacity, 1))))
+    return dict(r["best"])
 
 
 def apply(table, setting: Dict[str, int]) -> None:

@@ -114,7 +114,8 @@ struct Table {
     uint32_t split;
     uint32_t max_evictions;
     uint32_t flags;
-    uint32_t win_end;  // with kFlagMigrating: the window being split is [split, win_end)
+    uint32_t win_end;      // with kFlagMigrating: the window being split is [split, win_end)
+    uint32_t stash_depth;  // slots of a canonical stash that inserts may use (1..8)
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -1011,7 +1012,7 @@ __device__ __noinline__ uint8_t insert_locked(const Table& t, uint32_t k, u64 kv
         for (int q = 0; q < kRetryLimit; ++q) {
             Bucket S;
             load_bucket(Sp, S);
-            uint32_t se = empty_mask(S);
+            uint32_t se = empty_mask(S) & ((1u << t.stash_depth) - 1u);
             if (!se) {
                 if (!h1_first && b1 != b0) {
                     ev = try_evict_h1<P>(t, B1p, B1, b1, kv);

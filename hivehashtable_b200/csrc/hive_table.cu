@@ -78,7 +78,7 @@ struct hive_table {
     void* rbuf = nullptr;         // region-ordering buffers (13 bytes per op of the largest batch)
     uint64_t rcap = 0;
     int num_sms = 148;
-    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1, 1, 0};  // HIVE_TUNE_* knobs
+    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1, 1, 0, 8};  // HIVE_TUNE_* knobs
     bool tags_valid = true;  // the tag words match the slots (a zeroed table's do)
     void* ovf = nullptr;     // shrink: overflow entries of one merge step (kept between calls)
     size_t ovf_cap = 0;      // entries
@@ -1508,6 +1508,7 @@ int hive_create(const hive_config* cfg, hive_table** out) {
     }
     bind_arrays(h, block, nb_cap);
     h->t.max_evictions = (uint32_t)cfg->max_evictions;
+    h->t.stash_depth = (uint32_t)h->tune[HIVE_TUNE_STASH_DEPTH];
     h->t.flags = 0;
     set_geometry(h, 0, 0);
     *out = h;
@@ -2213,9 +2214,10 @@ int hive_debug_hold_lock(hive_table* h, uint64_t bucket, int held, void* stream)
 
 int hive_set_tuning(hive_table* h, int32_t key, int64_t value) {
     if (!valid_table(h) || key < 0 || key >= HIVE_NUM_TUNES) return HIVE_ERR_INVALID_ARG;
-    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0, 0, 0}, hi[HIVE_NUM_TUNES] = {2, 1, 8, 8, 2, 2, 2};
+    static const int64_t lo[HIVE_NUM_TUNES] = {0, 0, 0, 1, 0, 0, 0, 1}, hi[HIVE_NUM_TUNES] = {2, 1, 8, 8, 2, 2, 2, 8};
     if (value < lo[key] || value > hi[key]) return HIVE_ERR_INVALID_ARG;
     h->tune[key] = value;
+    if (key == HIVE_TUNE_STASH_DEPTH) h->t.stash_depth = (uint32_t)value;
     return HIVE_OK;
 }
 

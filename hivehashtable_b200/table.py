@@ -8,6 +8,7 @@ lib/libhive_b200.so and raises if that library is missing: there is no CPU fallb
 from __future__ import annotations
 
 import ctypes
+import os
 import warnings
 from pathlib import Path
 from typing import Optional, Tuple
@@ -40,7 +41,7 @@ COUNTER_NAMES = {0: "slow_path", 1: "evictions", 2: "stash_push", 3: "failed", 4
                  5: "retry_out", 6: "dup_fixed", 7: "lock_waits", 15: "error_bits"}
 # Launch-tuning knobs (HIVE_TUNE_*): how a batch runs, never what it computes
 TUNES = {"region_insert": 0, "region_find": 1, "subbatches": 2, "second_pass_blocks": 3, "bulk_retag": 4,
-         "tags": 5, "l2_window": 6}
+         "tags": 5, "l2_window": 6, "stash_depth": 7}
 
 # Policy names accepted by the reference's dispatcher (src/hive_dispatch.cu:829-871).  The
 # ones outside the hot path fall back to Default2Hash with a message, as the reference does for
@@ -187,7 +188,7 @@ class HiveHashTable:
     """
 
     def __init__(self, capacity: int, policy: str = "Default2Hash", max_evictions: int = 8,
-                 max_capacity: Optional[int] = None, device=None):
+                 max_capacity: Optional[int] = None, device=None, tuning=None):
         lib = library()
         if not torch.cuda.is_available():
             raise HiveError(7, "HiveHashTable")
@@ -197,12 +198,28 @@ class HiveHashTable:
         self.policy = policy
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
                                    else torch.device(device).index or 0)
+        # a tuned setting (hivehashtable_b200.autotune): a dict, or "cache" for the entry of this
+        # GPU / policy / nearest capacity in the HIVE_TUNE_CACHE file (used by default when set)
+        if tuning is None and os.environ.get("HIVE_TUNE_CACHE"):
+            tuning = "cache"
+        self.tuned = None
+        if tuning == "cache":
+            from .autotune import lookup_cached
+
+            self.tuned = lookup_cached(Path(os.environ.get("HIVE_TUNE_CACHE", "")), torch.cuda.get_device_name(self.device),
+                                       int(capacity), policy)
+        elif isinstance(tuning, dict):
+            self.tuned = dict(tuning)
+        if self.tuned and "max_evictions" in self.tuned:
+            max_evictions = int(self.tuned["max_evictions"])
         cfg = _Config(int(capacity), int(max_capacity or 0), POLICIES[policy], int(max_evictions),
                       self.device.index, 0)
         h = ctypes.c_void_p()
         _check(lib.hive_create(ctypes.byref(cfg), ctypes.byref(h)), "hive_create")
         self._h = h
         self._lib = lib
+        if self.tuned:
+            self.set_tuning(**{k: v for k, v in self.tuned.items() if k != "max_evictions"})
 
     # -- plumbing ---------------------------------------------------------------------------
     def _stream(self, stream=None) -> int:

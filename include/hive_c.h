@@ -314,7 +314,11 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
                                         covering as much as the limit allows.  Measured at 2^22
                                         slots (LF 0.9, L2 flushed between batches): 2% slower
                                         with the window, so it is off unless asked for           */
-#define HIVE_NUM_TUNES 7
+#define HIVE_TUNE_STASH_DEPTH 7      /* slots of a canonical bucket's overflow stash that inserts
+                                        may use, 1..8 (default 8, the reference's 8-slot stash,
+                                        include/hive_stash_table.cuh:20-27): fewer keep stash
+                                        reads shorter and leave more keys unplaced near LF 1     */
+#define HIVE_NUM_TUNES 8
 
 /* Set knob `key` to `value`.  HIVE_ERR_INVALID_ARG for an unknown key or a value out of range. */
 int hive_set_tuning(hive_table* t, int32_t key, int64_t value);

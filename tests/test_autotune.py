@@ -39,19 +39,43 @@ def test_search_rejects_settings_that_lose_inserts_or_answers():
     assert autotune.search(wrong)["best"]["tags"] != 0
 
 
+def test_cache_lookup_takes_the_nearest_capacity(tmp_path):
+    import json
+
+    cache = tmp_path / "tune.json"
+    entries = {}
+    for cap, spb in ((1 << 20, 2), (1 << 24, 8)):
+        best = dict(autotune.DEFAULTS, second_pass_blocks=spb)
+        entries[autotune.cache_key("GPU-X", cap, 0.9, 0.5, "Default2Hash")] = {
+            "best": best, "gpu": "GPU-X", "capacity_slots": cap, "policy": "Default2Hash"}
+    cache.write_text(json.dumps(entries))
+    assert autotune.lookup_cached(cache, "GPU-X", 1 << 21, "Default2Hash")["second_pass_blocks"] == 2
+    assert autotune.lookup_cached(cache, "GPU-X", 1 << 26, "Default2Hash")["second_pass_blocks"] == 8
+    assert autotune.lookup_cached(cache, "GPU-Y", 1 << 21, "Default2Hash") is None
+    assert autotune.lookup_cached(cache, "GPU-X", 1 << 21, "MurmurCityHash") is None
+    assert autotune.lookup_cached(tmp_path / "none.json", "GPU-X", 1 << 21, "Default2Hash") is None
+
+
 @pytest.mark.gpu
-def test_tuned_setting_keeps_results(cuda):
+def test_tuned_setting_keeps_results(cuda, tmp_path, monkeypatch):
+    """Tune on the GPU into a cache file; a table created with that cache in HIVE_TUNE_CACHE takes
+    the tuned knobs (and eviction bound) and still gives the replay's results."""
     import oracle
     from hivehashtable_b200 import HiveHashTable, u32
 
-    r = autotune.autotune(1 << 18, 0.9, reps=1, warmup=1)
+    cache = tmp_path / "tune.json"
+    r = autotune.autotune(1 << 18, 0.9, reps=1, warmup=1, cache=cache)
     best = r["best"]
     assert set(best) == set(autotune.DEFAULTS) and r["best_ms"] <= r["default_ms"] + 1e-9
     keys, absent, st = oracle.gen_keys(3, int(0.9 * (1 << 18)), 1 << 14)
     vals = oracle.values_for(keys)
     m = oracle.ReplayMap()
-    with HiveHashTable(1 << 18, max_evictions=best["max_evictions"]) as t:
-        autotune.apply(t, best)
+    monkeypatch.setenv("HIVE_TUNE_CACHE", str(cache))
+    with HiveHashTable(1 << 18) as t:
+        assert t.tuned == best
+        knobs = t.tuning()
+        assert all(knobs[k] == v for k, v in best.items() if k != "max_evictions")
+        assert t.info()["max_evictions"] == best["max_evictions"]
         s = t.insert(keys, vals).cpu().numpy()
         assert (s != 0).all()
         m.insert(keys, vals)
@@ -60,3 +84,7 @@ def test_tuned_setting_keeps_results(cuda):
         ev, ef = m.find(look)
         np.testing.assert_array_equal(f.cpu().numpy(), ef)
         np.testing.assert_array_equal(u32(v), ev)
+        gk, gv = t.dump()
+        ok, ov = m.dump()
+        np.testing.assert_array_equal(gk, ok)
+        np.testing.assert_array_equal(gv, ov)

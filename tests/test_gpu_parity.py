@@ -256,9 +256,9 @@ def test_tags_switched_off_and_on(cuda, policy):
 def test_tuning_bounds(cuda):
     with HiveHashTable(1 << 12) as t:
         assert t.tuning() == {"region_insert": 0, "region_find": 0, "subbatches": 0, "second_pass_blocks": 4,
-                              "bulk_retag": 1, "tags": 1, "l2_window": 0}
+                              "bulk_retag": 1, "tags": 1, "l2_window": 0, "stash_depth": 8}
         for bad in ({"region_insert": 3}, {"subbatches": 9}, {"second_pass_blocks": 0}, {"bulk_retag": 3},
-                    {"tags": 3}, {"l2_window": 3}):
+                    {"tags": 3}, {"l2_window": 3}, {"stash_depth": 0}, {"stash_depth": 9}):
             with pytest.raises(HiveError):
                 t.set_tuning(**bad)
         t.set_tuning(second_pass_blocks=8)
@@ -438,6 +438,26 @@ def test_forced_collisions_stash_and_overflow(cuda, max_ev):
         st2 = _insert_and_check(t, m, keys[:150], vals[:150] + np.uint32(1))
         assert (st2 != ST_FAIL).sum() > 0
         _find_and_check(t, m, np.concatenate([keys, absent]))
+        _assert_same_set(t, m)
+
+
+@pytest.mark.parametrize("depth", [1, 2, 4])
+def test_stash_depth_limits_the_stash(cuda, depth):
+    """HIVE_TUNE_STASH_DEPTH: forced collisions place at most `depth` keys in each canonical stash;
+    the placed set and every lookup still match the replay."""
+    keys, absent, _ = oracle.gen_keys(3, 300, 100)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(64) as t:
+        t.set_tuning(stash_depth=depth)
+        st = _insert_and_check(t, m, keys, vals)
+        assert 0 < (st == ST_STASHED).sum() <= depth * 8  # 8 buckets, `depth` stash slots each
+        _find_and_check(t, m, np.concatenate([keys, absent]))
+        _assert_same_set(t, m)
+        t.set_tuning(stash_depth=8)  # deeper stashes take the keys that found no room
+        more = keys[st == ST_FAIL]
+        st2 = _insert_and_check(t, m, more, oracle.values_for(more))
+        assert (st2 == ST_STASHED).sum() > 0
         _assert_same_set(t, m)
 
 
