@@ -575,6 +575,70 @@ def run_resize(args, dev):
     return out
 
 
+def run_sharded(args, rank, world, local, dev):
+    """The hash-partitioned table (hivehashtable_b200/sharded.py): each of the N ranks holds a
+    2^cap_log-slot shard and submits its own n = LF * 2^cap_log keys (seed 7 + 1000 * rank); one
+    step = clear every shard, sharded bulk insert, sharded bulk lookup (present fraction as the
+    headline), each through the owner exchange (all_to_all_single over NCCL, also at N = 1).
+    Weak scaling: value = 2 n N / the slowest rank's time."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from hivehashtable_b200 import HiveHashTable, as_device_u32, workload
+    from hivehashtable_b200.sharded import ShardedHiveTable
+
+    if not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29517")
+        dist.init_process_group("nccl", rank=rank, world_size=world, timeout=timedelta(seconds=300), device_id=dev)
+    cap = 1 << args.cap_log
+    n = int(args.lf * cap)
+    keys_h, vals_h, look_h = workload.bulk_workload(args.seed + 1000 * rank, n, args.present)
+    keys, vals, look = as_device_u32(keys_h, dev), as_device_u32(vals_h, dev), as_device_u32(look_h, dev)
+    shard = HiveHashTable(cap, args.policy)
+    tbl = ShardedHiveTable(shard, dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        shard.clear()
+        st = tbl.insert(keys, vals)
+        _, f = tbl.find(look)
+        return st, f
+
+    for _ in range(args.warmup):
+        st, f = step()
+    torch.cuda.synchronize()
+    assert bool((st != 0).all()) and int(f.sum()) == int(round(look_h.size * args.present))
+    dist.barrier()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = torch.tensor([a.elapsed_time(b)], device=dev, dtype=torch.float64)
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms.item())
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC + " (sharded table)", "value": round(2 * n * world * args.steps / (ms / 1e3) / 1e6, 2),
+                "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seeded uint32 keys/values)",
+                "config": dict(workload_config(args, world),
+                               parallelism=f"sharded: {world} rank(s), one 2^{args.cap_log}-slot shard each; owner = "
+                                           "(fmix32(key ^ 0x9E3779B9) * N) >> 32; one all_to_all_single of 9-byte "
+                                           "records out and 5-byte results back per call (NCCL)"),
+                "exchange_bytes_per_op": {"out": 9, "back": 5}}
+    shard.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    return line
+
+
 def workload_config(args, world):
     cap = 1 << args.cap_log
     n = int(args.lf * cap)
