@@ -41,7 +41,7 @@ COUNTER_NAMES = {0: "slow_path", 1: "evictions", 2: "stash_push", 3: "failed", 4
                  5: "retry_out", 6: "dup_fixed", 7: "lock_waits", 15: "error_bits"}
 # Launch-tuning knobs (HIVE_TUNE_*): how a batch runs, never what it computes
 TUNES = {"region_insert": 0, "region_find": 1, "subbatches": 2, "second_pass_blocks": 3, "bulk_retag": 4,
-         "tags": 5, "l2_window": 6, "stash_depth": 7}
+         "tags": 5, "l2_window": 6, "stash_depth": 7, "binned": 8}
 
 # Policy names accepted by the reference's dispatcher (src/hive_dispatch.cu:829-871).  The
 # ones outside the hot path fall back to Default2Hash with a message, as the reference does for
