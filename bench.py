@@ -456,7 +456,8 @@ def served_summary(dev, n_req=1 << 20, max_batch=1 << 14):
     C lookups, D 95 % lookups / 5 % new inserts; Zipf 0.99 over 2^26 preloaded records in 2^27
     slots), the closed-loop peak of the continuous loop (depth 4), then Poisson arrivals at 80 % of
     that peak through the continuous loop and through the plain loop (depth 1, one batch at a
-    time), with p50 / p99 / p999 latency from arrival to result on the host."""
+    time), with p50 / p99 / p999 latency from arrival to result on the host: of three runs, the
+    one with the median p99."""
     import torch
     from hivehashtable_b200 import HiveHashTable
     from hivehashtable_b200.serving import ServedWorkload, poisson_arrivals, serve
@@ -476,8 +477,12 @@ def served_summary(dev, n_req=1 << 20, max_batch=1 << 14):
             peak = run(poisson_arrivals(n_req, 0), 4)["mops"]
             row = {"peak_mops": round(peak, 2)}
             for name, depth in (("continuous_80", 4), ("plain_80", 1)):
-                r = run(poisson_arrivals(n_req, 0.8 * peak * 1e6, seed=80), depth)
-                row[name] = {k: round(r[k], 4) for k in ("mops", "p50_ms", "p99_ms", "p999_ms")}
+                # three runs with different arrival draws; the one with the median p99 is reported
+                # (a single host stall of a millisecond or two moves one run's p99)
+                rs = sorted((run(poisson_arrivals(n_req, 0.8 * peak * 1e6, seed=80 + j), depth) for j in range(3)),
+                            key=lambda r: r["p99_ms"])
+                row[name] = {k: round(rs[1][k], 4) for k in ("mops", "p50_ms", "p99_ms", "p999_ms")}
+                row[name]["p99_ms_runs"] = [round(r["p99_ms"], 4) for r in rs]
             out["mixes"][mix] = row
             t.check()
     return out

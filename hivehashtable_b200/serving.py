@@ -111,9 +111,13 @@ def serve(table: HiveHashTable, types, keys, vals, arrival, depth: int = 4, max_
     vals = np.ascontiguousarray(vals, dtype=np.uint32)
     arrival = np.ascontiguousarray(arrival, dtype=np.float64)
     n = keys.size
-    out_v = np.zeros(n, dtype=np.uint32)
-    out_s = np.zeros(n, dtype=np.uint8)
-    done = np.zeros(n, dtype=np.float64)
+    # written (not just allocated) before the loop: np.zeros maps zero pages lazily, and the page
+    # faults of first writes would land on the answering thread inside the timed loop
+    out_v = np.empty(n, dtype=np.uint32)
+    out_s = np.empty(n, dtype=np.uint8)
+    done = np.empty(n, dtype=np.float64)
+    for a in (out_v, out_s, done):
+        a.fill(0)
     if grow_start is None:
         grow_start = 0.8 * max_load
     cfg = ServeConfig(depth, max_batch, max_load, table.size() if live_keys is None else live_keys, grow_start)
