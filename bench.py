@@ -47,7 +47,7 @@ BYTES_LOOKUP_ABSENT = 140.0
 # at this workload (2^26 slots, LF 0.9, Default2Hash): the insert's three launches (first pass,
 # deferred pass, fingerprint rebuild) and k_find; profiles/bulk_insert_lookup_2p26_dram_traffic.txt.
 # A measurement of this build: re-capture after a change to either kernel.
-TRAFFIC_PER_OP = {"insert": 184.0, "lookup": 99.6}
+TRAFFIC_PER_OP = {"insert": 183.1, "lookup": 99.6}
 
 
 def parse_args():
@@ -68,7 +68,9 @@ def parse_args():
     ap.add_argument("--sharded", action="store_true",
                     help="bulk workload through the hash-partitioned table (exchange over NCCL) instead of replicas")
     ap.add_argument("--l2-window", type=int, choices=[0, 1, 2], default=None,
-                    help="HIVE_TUNE_L2_WINDOW for the table (default: the library's, 1)")
+                    help="HIVE_TUNE_L2_WINDOW for the table (default: the library's, 0)")
+    ap.add_argument("--binned", type=int, choices=[0, 1, 2], default=None,
+                    help="HIVE_TUNE_BINNED for the table (default: the library's, 0 = unbinned insert)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip the A/B against the reference's own GPU build")
     ap.add_argument("--workload", choices=["bulk", "batched", "served", "resize"], default="bulk",
@@ -78,11 +80,11 @@ def parse_args():
     return ap.parse_args()
 
 
-def launches_per_step(cap, n_ins, n_look):
-    """Kernels of this library launched per step with the default tuning (region ordering off):
-    clear (k_clear_stash), insert (first pass, deferred pass, the pass over the ops it handed on to
-    the stash, tag rebuild), lookup (k_find)."""
-    return 1 + 4 + 1
+def launches_per_step(cap, n_ins, n_look, binned=False):
+    """Kernels of this library launched per step (region ordering off): clear (k_clear_stash),
+    insert (first pass -- or, binned, histogram, scan, two partition passes, H0 and H1 stages --
+    the converged second pass, the pass over the ops it handed on, tag rebuild), lookup (k_find)."""
+    return 1 + (6 if binned else 1) + 3 + 1
 
 
 def load_peaks():
@@ -659,6 +661,8 @@ def workload_config(args, world):
         d["l2"] = f"inputs larger than L2 (table {cap * 8 >> 20} MiB, each key array {n * 4 / 1e6:.0f} MB); no flush"
     if getattr(args, "l2_window", None) is not None:
         d["l2_window"] = args.l2_window
+    if getattr(args, "binned", None):
+        d["binned_insert"] = args.binned
     return d
 
 
@@ -718,6 +722,8 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if fits_l2 else None
     if args.l2_window is not None:
         table.set_tuning(l2_window=args.l2_window)
+    if args.binned is not None:
+        table.set_tuning(binned=args.binned)
 
     def step(ev=None):
         if flush is not None:
@@ -833,7 +839,9 @@ def main():
         find_avg = sum(find_ms) / len(find_ms)
         lb = n_present * BYTES_LOOKUP_PRESENT + (n_look - n_present) * BYTES_LOOKUP_ABSENT
         kernels = {
-            "k_insert": {"ms": ins_avg, "bytes": n * BYTES_INSERT, "ops": n, "traffic_per_op": TRAFFIC_PER_OP["insert"]},
+            # the ncu traffic figure is the unbinned insert's
+            "k_insert": {"ms": ins_avg, "bytes": n * BYTES_INSERT, "ops": n,
+                         "traffic_per_op": None if args.binned else TRAFFIC_PER_OP["insert"]},
             "k_find": {"ms": find_avg, "bytes": lb, "ops": n_look, "traffic_per_op": TRAFFIC_PER_OP["lookup"]},
         }
         rl = {}
@@ -860,7 +868,9 @@ def main():
                     rl["k_insert"]["mops"] / 1e3 / ceiling["read64_cas_32MiB_l2"]["gops"], 4)
                 rl["k_find"]["frac_of_l2_probe_ops"] = round(
                     rl["k_find"]["mops"] / 1e3 / ceiling["read64_32MiB_l2"]["gops"], 4)
-        rl["k_insert"]["launches"] = ["k_insert", "k_insert_converged", "k_insert_deferred (handed-on ops)", "k_retag"]
+        rl["k_insert"]["launches"] = (["k_bin_count", "k_bin_scan", "k_bin_part_super", "k_bin_part_bin", "k_bin_h0",
+                                       "k_bin_h1"] if args.binned else ["k_insert"]) + \
+            ["k_insert_converged", "k_insert_deferred (handed-on ops)", "k_retag"]
         rl["k_find"]["launches"] = ["k_find"]
         dom = max(kernels, key=lambda k: kernels[k]["ms"])
         roof = dict(rl[dom], kernel="hive_insert" if dom == "k_insert" else dom)
@@ -870,7 +880,7 @@ def main():
                 "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seeded uint32 keys/values)",
                 "config": workload_config(args, world), "roofline": roof, "roofline_all": rl,
                 "insert_mops": rl["k_insert"]["mops"], "lookup_mops": rl["k_find"]["mops"],
-                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches_per_step(cap, n, n_look) * args.steps,
+                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches_per_step(cap, n, n_look, bool(args.binned)) * args.steps,
                 "insert_counters": step_counters, "random_bucket_ceiling": ceiling, "served": served,
                 "clocks": sampler.summary()}
         print(json.dumps(line), flush=True)
