@@ -47,7 +47,9 @@ BYTES_LOOKUP_ABSENT = 140.0
 # at this workload (2^26 slots, LF 0.9, Default2Hash): the insert's three launches (first pass,
 # deferred pass, fingerprint rebuild) and k_find; profiles/bulk_insert_lookup_2p26_dram_traffic.txt.
 # A measurement of this build: re-capture after a change to either kernel.
-TRAFFIC_PER_OP = {"insert": 183.1, "lookup": 99.6}
+# DRAM bytes per op from ncu (profiles/): the binned insert's from the 2^25-slot capture, whose
+# kernels' traffic grows with the ops and the table alike
+TRAFFIC_PER_OP = {"insert": 183.1, "insert_binned": 123.5, "lookup": 99.6}
 
 
 def parse_args():
@@ -70,7 +72,8 @@ def parse_args():
     ap.add_argument("--l2-window", type=int, choices=[0, 1, 2], default=None,
                     help="HIVE_TUNE_L2_WINDOW for the table (default: the library's, 0)")
     ap.add_argument("--binned", type=int, choices=[0, 1, 2], default=None,
-                    help="HIVE_TUNE_BINNED for the table (default: the library's, 0 = unbinned insert)")
+                    help="HIVE_TUNE_BINNED for the table (default: the library's, 1 = binned when the batch has "
+                         ">= 2^20 ops and one per bucket; 0 = the unbinned insert)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip the A/B against the reference's own GPU build")
     ap.add_argument("--workload", choices=["bulk", "batched", "served", "resize"], default="bulk",
@@ -661,8 +664,8 @@ def workload_config(args, world):
         d["l2"] = f"inputs larger than L2 (table {cap * 8 >> 20} MiB, each key array {n * 4 / 1e6:.0f} MB); no flush"
     if getattr(args, "l2_window", None) is not None:
         d["l2_window"] = args.l2_window
-    if getattr(args, "binned", None):
-        d["binned_insert"] = args.binned
+    if getattr(args, "binned", None) is not None:
+        d["binned_insert_knob"] = args.binned
     return d
 
 
@@ -724,6 +727,9 @@ def main():
         table.set_tuning(l2_window=args.l2_window)
     if args.binned is not None:
         table.set_tuning(binned=args.binned)
+    # which insert the batch takes (HIVE_TUNE_BINNED: 1 = batches of >= 2^20 ops and one per bucket)
+    tb = table.tuning()["binned"]
+    binned = tb == 2 or (tb == 1 and n >= (1 << 20) and n >= cap // 8)
 
     def step(ev=None):
         if flush is not None:
@@ -839,9 +845,8 @@ def main():
         find_avg = sum(find_ms) / len(find_ms)
         lb = n_present * BYTES_LOOKUP_PRESENT + (n_look - n_present) * BYTES_LOOKUP_ABSENT
         kernels = {
-            # the ncu traffic figure is the unbinned insert's
             "k_insert": {"ms": ins_avg, "bytes": n * BYTES_INSERT, "ops": n,
-                         "traffic_per_op": None if args.binned else TRAFFIC_PER_OP["insert"]},
+                         "traffic_per_op": TRAFFIC_PER_OP["insert_binned" if binned else "insert"]},
             "k_find": {"ms": find_avg, "bytes": lb, "ops": n_look, "traffic_per_op": TRAFFIC_PER_OP["lookup"]},
         }
         rl = {}
@@ -869,9 +874,10 @@ def main():
                 rl["k_find"]["frac_of_l2_probe_ops"] = round(
                     rl["k_find"]["mops"] / 1e3 / ceiling["read64_32MiB_l2"]["gops"], 4)
         rl["k_insert"]["launches"] = (["k_bin_count", "k_bin_scan", "k_bin_part_super", "k_bin_part_bin", "k_bin_h0",
-                                       "k_bin_h1"] if args.binned else ["k_insert"]) + \
+                                       "k_bin_h1"] if binned else ["k_insert"]) + \
             ["k_insert_converged", "k_insert_deferred (handed-on ops)", "k_retag"]
         rl["k_find"]["launches"] = ["k_find"]
+        rl["k_insert"]["insert_path"] = "binned" if binned else "unbinned"
         dom = max(kernels, key=lambda k: kernels[k]["ms"])
         roof = dict(rl[dom], kernel="hive_insert" if dom == "k_insert" else dom)
         line = {"metric": METRIC, "value": round(2 * n * args.steps * world / (ms / 1e3) / 1e6, 2), "unit": UNIT,
@@ -880,7 +886,7 @@ def main():
                 "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seeded uint32 keys/values)",
                 "config": workload_config(args, world), "roofline": roof, "roofline_all": rl,
                 "insert_mops": rl["k_insert"]["mops"], "lookup_mops": rl["k_find"]["mops"],
-                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches_per_step(cap, n, n_look, bool(args.binned)) * args.steps,
+                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches_per_step(cap, n, n_look, binned) * args.steps,
                 "insert_counters": step_counters, "random_bucket_ceiling": ceiling, "served": served,
                 "clocks": sampler.summary()}
         print(json.dumps(line), flush=True)

@@ -80,7 +80,7 @@ struct hive_table {
     void* bbuf = nullptr;         // binned-insert buffers (24 bytes per op of the largest batch)
     uint64_t bcap = 0;
     int num_sms = 148;
-    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1, 1, 0, 8, 0};  // HIVE_TUNE_* knobs
+    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1, 1, 0, 8, 1};  // HIVE_TUNE_* knobs
     bool tags_valid = true;  // the tag words match the slots (a zeroed table's do)
     void* ovf = nullptr;     // shrink: overflow entries of one merge step (kept between calls)
     size_t ovf_cap = 0;      // entries
@@ -453,7 +453,8 @@ constexpr uint32_t kMaxBins = 16384;                // 2^24 buckets; the histogr
 constexpr uint32_t kMaxSupers = kMaxBins / kSuperBins;
 constexpr int kBinBlock = 512;
 constexpr uint64_t kHistTile = (uint64_t)kBinBlock * 128;  // ops per block of the histogram
-constexpr uint32_t kPartTile = 8192;                       // ops staged per block of a partition pass
+constexpr uint32_t kPartPer = 8;                            // ops per thread of a partition pass
+constexpr uint32_t kPartTile = kBinBlock * kPartPer;        // ops staged per block of a partition pass
 constexpr uint64_t kBinMinOps = 1ull << 20;
 constexpr int kLoadBatch = 16;  // elements a thread loads before using any of them
 
@@ -573,115 +574,103 @@ struct PartSmem {
     uint32_t warp_sums[32];
 };
 
-// The tile's second half of a partition pass, after sm.cnt holds each destination's count:
-// reserve each destination's run of the output with one atomic on cursors[cur_base + d], place
-// every op (fetched again by get(e)) at its place in shared memory, then write the groups out
-// contiguously.  get(e) -> (kv, idx, digit) for tile element e, digit < 0 for no op.
-template <typename Get>
-__device__ __forceinline__ void part_place(PartSmem& sm, uint32_t ndig, uint32_t n_elems, uint32_t* cursors,
-                                           uint32_t cur_base, u64* __restrict__ out_kv,
-                                           uint32_t* __restrict__ out_idx, Get get) {
+// One tile of a partition pass.  Each thread holds kPartPer ops of the tile in registers (kv,
+// idx, destination d, -1 for none) and sm.cnt is zeroed.  Every op takes its rank in its group
+// from a shared-memory counter; each destination's run of the output is reserved with one
+// atomic on cursors[cur_base + d]; the ops are staged in shared memory in group order and the
+// groups written out contiguously.
+__device__ __forceinline__ void part_tile(PartSmem& sm, uint32_t ndig, const u64 (&kv)[kPartPer],
+                                          const uint32_t (&idx)[kPartPer], int (&d)[kPartPer],
+                                          uint32_t* cursors, uint32_t cur_base, u64* __restrict__ out_kv,
+                                          uint32_t* __restrict__ out_idx) {
+    // d[q] becomes (destination << 16) | rank (a tile holds fewer than 2^16 ops)
+#pragma unroll
+    for (int q = 0; q < (int)kPartPer; ++q)
+        if (d[q] >= 0) d[q] = (d[q] << 16) | (int)atomicAdd(sm.cnt + d[q], 1u);
     __syncthreads();
-    // exclusive scan of the counts (ndig <= 1024) and the global reservations
+    // exclusive scan of the counts (ndig <= kBinBlock threads) and the global reservations
     const uint32_t c = threadIdx.x < ndig ? sm.cnt[threadIdx.x] : 0u;
-    uint32_t ex = 0;
-    {
-        const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        uint32_t incl = c;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += y;
+    }
+    if (lane == 31) sm.warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kBinBlock / 32 ? sm.warp_sums[lane] : 0u;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= (unsigned)o) incl += y;
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (unsigned)o) w += y;
         }
-        if (lane == 31) sm.warp_sums[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t w = lane < kBinBlock / 32 ? sm.warp_sums[lane] : 0u;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= (unsigned)o) w += y;
-            }
-            if (lane < kBinBlock / 32) sm.warp_sums[lane] = w;
-        }
-        __syncthreads();
-        ex = incl - c + (warp ? sm.warp_sums[warp - 1] : 0u);
+        if (lane < kBinBlock / 32) sm.warp_sums[lane] = w;
     }
+    __syncthreads();
+    const uint32_t ex = incl - c + (warp ? sm.warp_sums[warp - 1] : 0u);
     if (threadIdx.x < ndig) {
         sm.lstart[threadIdx.x] = ex;
         sm.gbase[threadIdx.x] = c ? atomicAdd(cursors + cur_base + threadIdx.x, c) : 0u;
-        sm.cnt[threadIdx.x] = ex;  // from here on: the next free place of the group
+    }
+    if (threadIdx.x == kBinBlock - 1) sm.warp_sums[31] = ex + c;  // the tile's op count (ndig <= kBinBlock)
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < (int)kPartPer; ++q) {
+        if (d[q] < 0) continue;
+        const uint32_t g = (uint32_t)d[q] >> 16;
+        const uint32_t p = sm.lstart[g] + ((uint32_t)d[q] & 0xFFFFu);
+        sm.kv[p] = kv[q];
+        sm.idx[p] = idx[q];
+        sm.dig[p] = (uint8_t)g;
     }
     __syncthreads();
-    constexpr int kB = 8;
-    for (uint32_t e0 = threadIdx.x; e0 < n_elems; e0 += kB * kBinBlock) {
-        u64 kv[kB];
-        uint32_t idx[kB];
-        int d[kB];
-#pragma unroll
-        for (int q = 0; q < kB; ++q) {
-            const uint32_t e = e0 + q * kBinBlock;
-            d[q] = -1;
-            if (e < n_elems) get(e, kv[q], idx[q], d[q]);
-        }
-#pragma unroll
-        for (int q = 0; q < kB; ++q) {
-            if (d[q] < 0) continue;
-            const uint32_t p = atomicAdd(sm.cnt + d[q], 1u);
-            sm.kv[p] = kv[q];
-            sm.idx[p] = idx[q];
-            sm.dig[p] = (uint8_t)d[q];
-        }
-    }
-    __syncthreads();
-    const uint32_t total = sm.cnt[ndig - 1];
+    const uint32_t total = sm.warp_sums[31];
     for (uint32_t p = threadIdx.x; p < total; p += kBinBlock) {
-        const uint32_t d = sm.dig[p];
-        const uint32_t g = sm.gbase[d] + (p - sm.lstart[d]);
-        __stcg(out_kv + g, sm.kv[p]);
-        __stcg(out_idx + g, sm.idx[p]);
+        const uint32_t g = sm.dig[p];
+        const uint32_t at = sm.gbase[g] + (p - sm.lstart[g]);
+        __stcg(out_kv + at, sm.kv[p]);
+        __stcg(out_idx + at, sm.idx[p]);
     }
 }
 
 // First partition pass: keys and values -> (akv, aidx) grouped by super-bin; statuses
 // provisionally kStInserted (key 0: kStFail, an insert of key 0 is refused).
 template <int P>
-__global__ void __launch_bounds__(kBinBlock, 2) k_bin_part_super(hive::Table t, const uint32_t* __restrict__ keys,
+__global__ void __launch_bounds__(kBinBlock, 3) k_bin_part_super(hive::Table t, const uint32_t* __restrict__ keys,
                                                                   const uint32_t* __restrict__ vals, uint64_t n,
                                                                   Bins b, uint8_t* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char part_raw[];
     PartSmem& sm = *reinterpret_cast<PartSmem*>(part_raw);
-    for (uint32_t d = threadIdx.x; d < b.nsupers; d += kBinBlock) sm.cnt[d] = 0;
-    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < b.nsupers; x += kBinBlock) sm.cnt[x] = 0;
     const uint64_t lo = (uint64_t)blockIdx.x * kPartTile;
-    const uint32_t m = (uint32_t)(n - lo < kPartTile ? n - lo : kPartTile);
-    for (uint32_t e0 = threadIdx.x; e0 < m; e0 += kLoadBatch * kBinBlock) {
-        uint32_t kk[kLoadBatch];
+    u64 kv[kPartPer];
+    uint32_t idx[kPartPer];
+    int d[kPartPer];
+    uint32_t kk[kPartPer], vv[kPartPer];
 #pragma unroll
-        for (int q = 0; q < kLoadBatch; ++q) {
-            const uint32_t e = e0 + q * kBinBlock;
-            kk[q] = e < m ? __ldcg(keys + lo + e) : 0u;
-        }
-#pragma unroll
-        for (int q = 0; q < kLoadBatch; ++q) {
-            const uint32_t e = e0 + q * kBinBlock;
-            if (e >= m) continue;
-            if (status) __stcs(status + lo + e, kk[q] ? hive::kStInserted : hive::kStFail);
-            if (kk[q]) atomicAdd(sm.cnt + (bin_of<P>(t, kk[q]) >> kSuperShift), 1u);
-        }
+    for (int q = 0; q < (int)kPartPer; ++q) {  // every load of the tile first
+        const uint64_t i = lo + (uint64_t)q * kBinBlock + threadIdx.x;
+        kk[q] = i < n ? __ldcs(keys + i) : 0u;
+        vv[q] = i < n ? __ldcs(vals + i) : 0u;
     }
-    part_place(sm, b.nsupers, m, b.supcur, 0u, b.akv, b.aidx, [&](uint32_t e, u64& kv, uint32_t& idx, int& d) {
-        const uint32_t k = __ldcs(keys + lo + e);
-        d = k ? (int)(bin_of<P>(t, k) >> kSuperShift) : -1;
-        kv = k ? hive::pack(k, __ldcs(vals + lo + e)) : 0ull;
-        idx = (uint32_t)(lo + e);
-    });
+#pragma unroll
+    for (int q = 0; q < (int)kPartPer; ++q) {
+        const uint64_t i = lo + (uint64_t)q * kBinBlock + threadIdx.x;
+        if (i < n && status) __stcs(status + i, kk[q] ? hive::kStInserted : hive::kStFail);
+        d[q] = i < n && kk[q] ? (int)(bin_of<P>(t, kk[q]) >> kSuperShift) : -1;
+        kv[q] = hive::pack(kk[q], vv[q]);
+        idx[q] = (uint32_t)i;
+    }
+    __syncthreads();  // counters zeroed
+    part_tile(sm, b.nsupers, kv, idx, d, b.supcur, 0u, b.akv, b.aidx);
 }
 
 // Second partition pass: one tile of one super-bin's range of (akv, aidx) -> (rkv, ridx) grouped
 // by bin.  Blocks beyond the tile count do nothing.
 template <int P>
-__global__ void __launch_bounds__(kBinBlock, 2) k_bin_part_bin(hive::Table t, Bins b) {
+__global__ void __launch_bounds__(kBinBlock, 3) k_bin_part_bin(hive::Table t, Bins b) {
     extern __shared__ __align__(16) unsigned char part_raw[];
     PartSmem& sm = *reinterpret_cast<PartSmem*>(part_raw);
     if (blockIdx.x >= *b.ntiles) return;
@@ -689,24 +678,21 @@ __global__ void __launch_bounds__(kBinBlock, 2) k_bin_part_bin(hive::Table t, Bi
     const uint32_t lo = tile.x, m = tile.y - tile.x, sup = tile.z;
     const uint32_t first = sup * kSuperBins;
     const uint32_t ndig = min(kSuperBins, b.nbins - first);
-    for (uint32_t d = threadIdx.x; d < ndig; d += kBinBlock) sm.cnt[d] = 0;
-    __syncthreads();
-    for (uint32_t e0 = threadIdx.x; e0 < m; e0 += kLoadBatch * kBinBlock) {
-        uint32_t kk[kLoadBatch];
+    for (uint32_t x = threadIdx.x; x < ndig; x += kBinBlock) sm.cnt[x] = 0;
+    u64 kv[kPartPer];
+    uint32_t idx[kPartPer];
+    int d[kPartPer];
 #pragma unroll
-        for (int q = 0; q < kLoadBatch; ++q) {
-            const uint32_t e = e0 + q * kBinBlock;
-            kk[q] = e < m ? hive::key_of(__ldcg(b.akv + lo + e)) : 0u;
-        }
-#pragma unroll
-        for (int q = 0; q < kLoadBatch; ++q)
-            if (e0 + q * kBinBlock < m) atomicAdd(sm.cnt + (bin_of<P>(t, kk[q]) - first), 1u);
+    for (int q = 0; q < (int)kPartPer; ++q) {
+        const uint32_t e = q * kBinBlock + threadIdx.x;
+        kv[q] = e < m ? __ldcs(b.akv + lo + e) : 0ull;
+        idx[q] = e < m ? __ldcs(b.aidx + lo + e) : 0u;
     }
-    part_place(sm, ndig, m, b.bincur, first, b.rkv, b.ridx, [&](uint32_t e, u64& kv, uint32_t& idx, int& d) {
-        kv = __ldcs(b.akv + lo + e);
-        idx = __ldcs(b.aidx + lo + e);
-        d = (int)(bin_of<P>(t, hive::key_of(kv)) - first);
-    });
+#pragma unroll
+    for (int q = 0; q < (int)kPartPer; ++q)
+        d[q] = q * kBinBlock + threadIdx.x < m ? (int)(bin_of<P>(t, hive::key_of(kv[q])) - first) : -1;
+    __syncthreads();  // counters zeroed
+    part_tile(sm, ndig, kv, idx, d, b.bincur, first, b.rkv, b.ridx);
 }
 
 // The bin's slots in shared memory.  A bucket is 64 bytes, half a row of the 32 four-byte banks,
@@ -1704,13 +1690,14 @@ struct Regions {
     uint8_t* rst = nullptr;
 };
 
-// A bulk insert runs binned (HIVE_TUNE_BINNED: 0 (default) never, 1 for batches of at least 2^20
+// A bulk insert runs binned (HIVE_TUNE_BINNED: 0 never, 1 (default) for batches of at least 2^20
 // ops and one op per bucket, 2 whenever allowed) into a table without holes or a split in
 // progress, with the tag words rebuilt after the batch (or unused), and at most kMaxBins bins.
-// Measured at 2^26 slots, LF 0.9 (60.4 M ops): 3.47 ms against 3.45 ms unbinned.  The H0 and H1
-// stages take 1.17 ms where the unbinned first pass takes 2.72 ms, but the histogram and the two
-// partition passes take 1.3 ms, and the locked passes 0.97 ms against 0.55 ms: with every H0
-// claim first, 2.9 M ops reach them instead of 2.4 M, and they evict from H1 before the stash.
+// Measured at 2^26 slots, LF 0.9 (60.4 M ops): 3.08 ms against 3.45 ms unbinned, 124 against 183
+// DRAM bytes per op.  The histogram and the two partition passes take 0.91 ms, the H0 and H1
+// stages 1.16 ms where the unbinned first pass takes 2.72 ms, and the locked passes 0.94 ms
+// against 0.55 ms: with every H0 claim first, 2.9 M ops reach them instead of 2.4 M, and they
+// evict from H1 before the stash.
 bool use_bins(const hive_table* h, uint64_t n, const hive::Table& tv) {
     const int64_t m = h->tune[HIVE_TUNE_BINNED];
     const uint64_t nb = num_buckets(h);
@@ -1771,6 +1758,7 @@ int bin_passes(hive_table* h, const hive::Table& t, const Bins& b, const Defer& 
                const uint32_t* vals, uint64_t n, uint8_t* status, cudaStream_t s) {
     static_assert((size_t)kMaxBins * 4 <= 64 * 1024, "the histogram fits 64 KiB");
     static_assert(kMaxSupers <= 1024 && kMaxPartDigits <= kBinBlock, "one thread per destination");
+    static_assert(kPartTile < (1u << 16) && kMaxPartDigits <= 256, "rank and destination pack into an int");
     const unsigned hist_tiles = (unsigned)((n + kHistTile - 1) / kHistTile);
     const unsigned part_tiles = (unsigned)((n + kPartTile - 1) / kPartTile);
     const size_t hist_bytes = (size_t)b.nbins * 4;
@@ -2219,8 +2207,9 @@ int hive_insert(hive_table* h, const uint32_t* keys, const uint32_t* values, uin
         if (rc) return rc;
         // Every H1 claim came after every H0 claim, so the locked passes meet buckets that hold
         // all their primaries: they try H1's own keys as victims before the stash, which keeps
-        // the stashes from overflowing near LF 1 (a sequential model of this placement leaves 0
-        // of 2^24 keys unplaced at LF 1.0 this way, 33 with the stash first).
+        // the stashes from overflowing (a sequential model of this placement leaves 0 of 2^24 keys
+        // unplaced at LF 1.0 this way, 33 with the stash first; with the stash first, one key of
+        // 2^24 slots at LF 0.9 was left unplaced on the GPU).
         tt.flags |= hive::kFlagEvictH1;
         // the deferred queue is in bin order (the H1 stage reads its queue in the order the bins
         // filled it): visited in that order, the locked passes' warps would crowd onto the locks

@@ -324,10 +324,10 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
                                         (one read and one write of every bucket per batch instead
                                         of a random read and CAS per op); the ops whose canonical
                                         bucket is full continue as in the unbinned insert.  0
-                                        (default) never; 1 for batches of at least 2^20 ops and
+                                        never; 1 (default) for batches of at least 2^20 ops and
                                         one op per bucket; 2 whenever the table allows it.
-                                        Measured at 2^26 slots, LF 0.9: as fast as the unbinned
-                                        insert (3.47 against 3.45 ms), so it is off unless asked */
+                                        Measured at 2^26 slots, LF 0.9: 3.08 ms against 3.45 ms
+                                        for the unbinned insert                                 */
 #define HIVE_NUM_TUNES 9
 
 /* Set knob `key` to `value`.  HIVE_ERR_INVALID_ARG for an unknown key or a value out of range. */
