@@ -727,9 +727,11 @@ def main():
         table.set_tuning(l2_window=args.l2_window)
     if args.binned is not None:
         table.set_tuning(binned=args.binned)
-    # which insert the batch takes (HIVE_TUNE_BINNED: 1 = batches of >= 2^20 ops and one per bucket)
+    # which insert the batch takes (HIVE_TUNE_BINNED: 1 = batches of >= 2^20 ops and one per bucket
+    # into a table whose slots span at least three times the L2)
     tb = table.tuning()["binned"]
-    binned = tb == 2 or (tb == 1 and n >= (1 << 20) and n >= cap // 8)
+    l2 = torch.cuda.get_device_properties(dev).L2_cache_size
+    binned = tb == 2 or (tb == 1 and n >= (1 << 20) and n >= cap // 8 and cap * 8 >= 3 * l2)
 
     def step(ev=None):
         if flush is not None:

@@ -325,9 +325,11 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
                                         of a random read and CAS per op); the ops whose canonical
                                         bucket is full continue as in the unbinned insert.  0
                                         never; 1 (default) for batches of at least 2^20 ops and
-                                        one op per bucket; 2 whenever the table allows it.
-                                        Measured at 2^26 slots, LF 0.9: 3.08 ms against 3.45 ms
-                                        for the unbinned insert                                 */
+                                        one op per bucket into a table whose slots span at least
+                                        three times the L2 (2^26 slots and up on B200); 2
+                                        whenever the table allows it.  Measured at 2^26 slots,
+                                        LF 0.9: 3.08 ms against 3.45 ms for the unbinned insert;
+                                        at 2^25 slots 1.89 against 1.62 ms                      */
 #define HIVE_NUM_TUNES 9
 
 /* Set knob `key` to `value`.  HIVE_ERR_INVALID_ARG for an unknown key or a value out of range. */

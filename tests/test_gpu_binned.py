@@ -149,13 +149,13 @@ def test_binned_ragged_last_bin_and_crowded_bins(cuda, policy):
 
 @pytest.mark.parametrize("policy", POLICIES)
 def test_binned_and_unbinned_agree(cuda, policy):
-    """The automatic choice (binned=1) at 2^22 slots, LF 0.9 (binned: 3.8 M ops >= one per bucket),
-    and the unbinned insert: both place every key, same key->value set, both clean."""
+    """The binned insert (forced) and the unbinned insert at 2^22 slots, LF 0.9: both place every
+    key, same key->value set, both clean."""
     cap = 1 << 22
     keys, _, _ = oracle.gen_keys(9, int(0.9 * cap), 0)
     vals = oracle.values_for(keys)
     out = []
-    for binned in (1, 0):
+    for binned in (2, 0):
         with HiveHashTable(cap, policy) as t:
             t.set_tuning(binned=binned)
             st = _np(t.insert(keys, vals))
@@ -186,3 +186,21 @@ def test_binned_host_and_stream_calls(cuda):
             v, f = t.find(kd)
             assert bool(f.all()) and torch.equal(v, vd)
             assert t.verify() == CLEAN
+
+
+@pytest.mark.parametrize("policy", POLICIES)
+@pytest.mark.parametrize("lf", [0.9, 1.0])
+def test_binned_2p24(cuda, policy, lf):
+    """The binned insert (forced) at 2^24 slots, LF 0.9 and 1.0: every status and the full
+    key->value set equal the replay's; none unplaced at 0.9."""
+    cap = 1 << 24
+    keys, absent, _ = oracle.gen_keys(17, int(lf * cap), 1 << 16)
+    vals = oracle.values_for(keys)
+    m = oracle.ReplayMap()
+    with HiveHashTable(cap, policy) as t:
+        t.set_tuning(binned=2)
+        st = _insert_and_check(t, m, keys, vals)
+        if lf <= 0.9:
+            assert (st != ST_FAIL).all()
+        _lookups_match(t, m, keys, absent)
+        _same_set(t, m)
