@@ -261,6 +261,41 @@ __device__ __forceinline__ void defer_push(const Defer& d, bool deferred, uint64
     }
 }
 
+// defer_push for a whole block (every thread of the block calls it once): the block's deferred ops
+// are gathered in shared memory and appended to the queue with one atomic per block.  The queue
+// counter is one word, and a warp atomic on it for each warp holding a deferred op (1.4 M of them
+// in a bulk insert of 60 M ops) serialises on its L2 slice.
+__device__ __forceinline__ void block_defer_push(const Defer& d, bool deferred, uint64_t i, u64 kv) {
+    __shared__ uint32_t n_q;
+    __shared__ u64 q_at;
+    __shared__ uint32_t q_idx[kBlock];
+    __shared__ u64 q_kv[kBlock];
+    if (threadIdx.x == 0) n_q = 0;
+    __syncthreads();
+    const unsigned m = __ballot_sync(0xffffffffu, deferred);
+    if (m) {
+        const unsigned lane = threadIdx.x & 31;
+        const int leader = __ffs(m) - 1;
+        uint32_t at = 0;
+        if ((int)lane == leader) at = atomicAdd(&n_q, (uint32_t)__popc(m));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (deferred) {
+            const uint32_t pos = at + __popc(m & ((1u << lane) - 1u));
+            q_idx[pos] = (uint32_t)i;
+            q_kv[pos] = kv;
+        }
+    }
+    __syncthreads();
+    const uint32_t c = n_q;
+    if (!c) return;  // the same for every thread of the block
+    if (threadIdx.x == 0) q_at = atomicAdd(d.n, (u64)c);
+    __syncthreads();
+    if (threadIdx.x < c) {
+        d.q[q_at + threadIdx.x] = q_idx[threadIdx.x];
+        if (d.kv) d.kv[q_at + threadIdx.x] = q_kv[threadIdx.x];
+    }
+}
+
 // First pass (kDefer) or the whole protocol in one pass (!kDefer, batches too large to queue)
 // over ops [lo, hi) of the batch; deferred ops are queued by their index in the batch, so the
 // first passes of several chunks of one batch feed one second pass.
@@ -271,8 +306,9 @@ __global__ void __launch_bounds__(kBlock, (kDefer && hive::mode_base(kMode) == h
     const uint64_t i = lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < hi;
     uint8_t st = hive::kStFail;
-    if constexpr (kDefer && hive::mode_base(kMode) == hive::kModeMono && (kMode & hive::kModeUntagged) &&
-                  !(kMode & hive::kModePrimary)) {
+    constexpr bool kCoop = kDefer && hive::mode_base(kMode) == hive::kModeMono && (kMode & hive::kModeUntagged) &&
+                           !(kMode & hive::kModePrimary);
+    if constexpr (kCoop) {
         // Bulk first pass, one op per thread: each bucket read is one request shared by a lane
         // pair (every lane of the warp takes part, so nothing here returns early).
         const uint32_t k = active ? __ldcs(keys + i) : 0u;
@@ -287,14 +323,17 @@ __global__ void __launch_bounds__(kBlock, (kDefer && hive::mode_base(kMode) == h
         const uint32_t m1 = hive::warp_bucket_masks(t.slots, need1, b1, k);
         if (need1) st = hive::claim_from_masks(t, b1, k, kv, m1);
         if (live && !st) st = hive::kStDefer;
+        block_defer_push(d, st == hive::kStDefer, i, kv);
     } else if (active) {
         st = hive::insert_one<P, kDefer, kMode>(t, __ldcs(keys + i), __ldcs(vals + i));
     }
-    // a deferred op's key and value are read again (L2 hits: the lines were just streamed in)
-    // rather than kept live across the insert
-    u64 kv = 0;
-    if (kDefer && st == hive::kStDefer && d.kv) kv = hive::pack(__ldcg(keys + i), __ldcg(vals + i));
-    if (kDefer) defer_push(d, st == hive::kStDefer, i, kv);
+    if constexpr (kDefer && !kCoop) {
+        // a deferred op's key and value are read again (L2 hits: the lines were just streamed in)
+        // rather than kept live across the insert
+        u64 kv = 0;
+        if (st == hive::kStDefer && d.kv) kv = hive::pack(__ldcg(keys + i), __ldcg(vals + i));
+        defer_push(d, st == hive::kStDefer, i, kv);
+    }
     // a deferred op's provisional status (Defer::kv) is kStInserted
     if (active && status && (st != hive::kStDefer || d.kv)) __stcs(status + i, st == hive::kStDefer ? hive::kStInserted : st);
 }
