@@ -187,7 +187,7 @@ class ShardedHiveTable:
         receives with its bulk insert."""
         t = self.local
         bulk = None if t is None else (lambda _t, k, v: (t.insert(k, v), torch.zeros_like(k)))
-        return self.apply(torch.zeros(len(keys), dtype=torch.uint8), keys, vals, bulk)[0]
+        return self.apply(torch.zeros(len(keys), dtype=torch.uint8, device=self.device), keys, vals, bulk)[0]
 
     def find(self, keys):
         """Bulk lookup: (values, found).  A HiveHashTable shard answers with its bulk find."""
@@ -197,6 +197,9 @@ class ShardedHiveTable:
             v, f = t.find(k)
             return f, v
 
-        st, ov = self.apply(torch.ones(len(keys), dtype=torch.uint8), keys, torch.zeros(len(keys), dtype=torch.int32),
+        # op types and the (unused) values are made where the exchange runs: built on the host they
+        # would cross PCIe on every call
+        n, d = len(keys), self.device
+        st, ov = self.apply(torch.ones(n, dtype=torch.uint8, device=d), keys, torch.zeros(n, dtype=torch.int32, device=d),
                             None if t is None else bulk)
         return ov, st
