@@ -33,9 +33,9 @@ import json
 from pathlib import Path
 from typing import Callable, Dict, Optional
 
-DEFAULTS = {"tags": 1, "region_insert": 0, "second_pass_blocks": 4, "max_evictions": 8, "stash_depth": 8,
+DEFAULTS = {"tags": 1, "region_insert": 0, "second_pass_blocks": 8, "max_evictions": 8, "stash_depth": 8,
             "l2_window": 0, "binned": 1}
-SPACE = {"tags": [1, 0, 2], "region_insert": [0, 2], "second_pass_blocks": [4, 2, 8], "max_evictions": [8, 4],
+SPACE = {"tags": [1, 0, 2], "region_insert": [0, 2], "second_pass_blocks": [8, 4, 2], "max_evictions": [8, 4],
          "stash_depth": [8, 4], "l2_window": [0, 1], "binned": [1, 0]}
 
 # measure(setting) -> {"ms": float, "failed": int, "correct": bool}

@@ -81,7 +81,7 @@ struct hive_table {
     uint64_t bcap = 0;
     int num_sms = 148;
     int l2_bytes = 126 << 20;  // the device's L2 (cudaDevAttrL2CacheSize)
-    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 4, 1, 1, 0, 8, 1};  // HIVE_TUNE_* knobs
+    int64_t tune[HIVE_NUM_TUNES] = {0, 0, 0, 8, 1, 1, 0, 8, 1};  // HIVE_TUNE_* knobs
     bool tags_valid = true;  // the tag words match the slots (a zeroed table's do)
     void* ovf = nullptr;     // shrink: overflow entries of one merge step (kept between calls)
     size_t ovf_cap = 0;      // entries
@@ -1764,11 +1764,11 @@ struct Regions {
 // unbinned insert's random accesses are served there and the partition passes do not pay:
 // binned 0.44 ms against 0.27 ms at 2^22 slots (32 MiB), 1.89 against 1.62 ms at 2^25 (256 MiB,
 // twice the L2).
-// Measured at 2^26 slots, LF 0.9 (60.4 M ops): 3.08 ms against 3.45 ms unbinned, 124 against 183
+// Measured at 2^26 slots, LF 0.9 (60.4 M ops): 2.89 ms against 3.26 ms unbinned, 124 against 183
 // DRAM bytes per op.  The histogram and the two partition passes take 0.91 ms, the H0 and H1
-// stages 1.16 ms where the unbinned first pass takes 2.72 ms, and the locked passes 0.94 ms
-// against 0.55 ms: with every H0 claim first, 2.9 M ops reach them instead of 2.4 M, and they
-// evict from H1 before the stash.
+// stages about 1.0 ms where the unbinned first pass takes about 2.6 ms, and the locked passes
+// more than the unbinned insert's: with every H0 claim first, 2.9 M ops reach them instead of
+// 2.4 M, and they evict from H1 before the stash.
 bool use_bins(const hive_table* h, uint64_t n, const hive::Table& tv) {
     const int64_t m = h->tune[HIVE_TUNE_BINNED];
     const uint64_t nb = num_buckets(h);

@@ -297,7 +297,8 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
 #define HIVE_TUNE_SUBBATCHES 2       /* sub-batches of a region-ordered insert, 1..8; 0 (default)
                                         = chosen from the share of the capacity the batch adds   */
 #define HIVE_TUNE_SECOND_PASS_BLOCKS 3 /* resident blocks per SM of the second insert pass, 1..8;
-                                          default 4                                             */
+                                          default 8 (the autotuner's choice at 2^26 slots, LF 0.9:
+                                          4.10 against 4.21 ms per insert + lookup with 4)      */
 #define HIVE_TUNE_BULK_RETAG 4       /* per-slot fingerprint upkeep of hive_insert*: 0 per op; 1
                                         (default) per op for batches under one op per eight
                                         buckets, else one rebuild of the fingerprints after the
@@ -328,7 +329,7 @@ int hive_verify(hive_table* t, uint64_t* out, void* stream);
                                         one op per bucket into a table whose slots span at least
                                         three times the L2 (2^26 slots and up on B200); 2
                                         whenever the table allows it.  Measured at 2^26 slots,
-                                        LF 0.9: 3.08 ms against 3.45 ms for the unbinned insert;
+                                        LF 0.9: 2.89 ms against 3.26 ms for the unbinned insert;
                                         at 2^25 slots 1.89 against 1.62 ms                      */
 #define HIVE_NUM_TUNES 9
 

@@ -19,9 +19,9 @@ def _fake(costs, bad=()):
 
 
 def test_search_takes_the_fastest_valid_setting():
-    measure, calls = _fake({("tags", 2): 1.0, ("second_pass_blocks", 8): 0.5, ("max_evictions", 4): -0.5})
+    measure, calls = _fake({("tags", 2): 1.0, ("second_pass_blocks", 4): 0.5, ("max_evictions", 4): -0.5})
     r = autotune.search(measure)
-    assert r["best"] == dict(autotune.DEFAULTS, tags=2, second_pass_blocks=8)
+    assert r["best"] == dict(autotune.DEFAULTS, tags=2, second_pass_blocks=4)
     assert r["best_ms"] == pytest.approx(8.5) and r["default_ms"] == pytest.approx(10.0)
     # each setting measured once
     keys = [tuple(sorted(c.items())) for c in calls]

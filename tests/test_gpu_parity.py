@@ -255,13 +255,13 @@ def test_tags_switched_off_and_on(cuda, policy):
 
 def test_tuning_bounds(cuda):
     with HiveHashTable(1 << 12) as t:
-        assert t.tuning() == {"region_insert": 0, "region_find": 0, "subbatches": 0, "second_pass_blocks": 4,
+        assert t.tuning() == {"region_insert": 0, "region_find": 0, "subbatches": 0, "second_pass_blocks": 8,
                               "bulk_retag": 1, "tags": 1, "l2_window": 0, "stash_depth": 8, "binned": 1}
         for bad in ({"region_insert": 3}, {"subbatches": 9}, {"second_pass_blocks": 0}, {"bulk_retag": 3},
                     {"tags": 3}, {"l2_window": 3}, {"stash_depth": 0}, {"stash_depth": 9}, {"binned": 3}):
             with pytest.raises(HiveError):
                 t.set_tuning(**bad)
-        t.set_tuning(second_pass_blocks=8)
+        t.set_tuning(second_pass_blocks=2)
         keys, _, _ = oracle.gen_keys(3, 3000, 0)
         m = oracle.ReplayMap()
         _insert_and_check(t, m, keys, oracle.values_for(keys))
