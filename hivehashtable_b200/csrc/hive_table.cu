@@ -854,12 +854,19 @@ __global__ void __launch_bounds__(kBinBlock) k_bin_h0(hive::Table t, Bins b, uin
     }
     __syncthreads();
     if (threadIdx.x == 0) b.ocnt[blockIdx.x] = n_over;
-    // full hints (a bin starts on a multiple of 32 buckets, so each warp owns whole words)
+    // full hints (a bin starts on a multiple of 32 buckets, so each warp owns whole words).  Each
+    // lane reads its bucket's four 16-byte chunks in swizzled order, which keeps the 8 lanes of a
+    // shared-memory phase on 8 different bank groups (8-byte reads of consecutive buckets put
+    // every other lane on the same banks: a 16-way conflict).
+    const uint4* cv = reinterpret_cast<const uint4*>(slab);
     for (uint32_t g = threadIdx.x; g < ((nbk + 31) & ~31u); g += kBinBlock) {
         bool full = g < nbk;
         if (full) {
 #pragma unroll
-            for (int j = 0; j < hive::kSlots; ++j) full = full && slab[(size_t)g * hive::kSlots + j] != 0ull;
+            for (uint32_t q = 0; q < 4; ++q) {
+                const uint4 c = cv[slab_chunk(g, q)];
+                full = full && (c.x | c.y) && (c.z | c.w);
+            }
         }
         const unsigned fm = __ballot_sync(0xffffffffu, full);
         if ((threadIdx.x & 31) == 0 && fm) atomicOr(t.full_bits + ((b_lo + g) >> 5), fm);
